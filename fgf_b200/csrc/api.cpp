@@ -1,0 +1,794 @@
+// api.cpp -- the C ABI of libfgfcuda.so (include/fgf_cuda.h).
+//
+// Each entry point validates its arguments in the same order, and with the
+// same message text, as the matching `fgf::ops` function (src/ops.rs), applies
+// the same zero/one shortcuts, and then lowers the call to launches of the
+// matrix kernel: rows[j] (^)= XOR_t c[t][j] * src_t.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fgf_cuda.h"
+#include "internal.hpp"
+
+using namespace fgfc;
+
+namespace {
+
+thread_local std::string t_err;
+
+fgfc_status fail(fgfc_status st, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  t_err = buf;
+  return st;
+}
+
+fgfc_status ok() {
+  t_err.clear();
+  return FGFC_OK;
+}
+
+fgfc_status cuda_fail(cudaError_t e, const char* what) {
+  return fail(FGFC_ERR_CUDA, "%s: CUDA error: %s", what, cudaGetErrorString(e));
+}
+
+bool valid_field(int f) { return f >= 0 && f <= 3; }
+
+size_t zu(size_t v) { return v; }
+
+// ops.rs:300-307
+bool check_width(int f, const char* name, size_t len, fgfc_status* st) {
+  if (len % field_bytes(f) != 0) {
+    *st = fail(FGFC_ERR_WIDTH, "%s: buffer of %zu bytes is not a whole number of %s elements", name,
+               len, field_name(f));
+    return false;
+  }
+  return true;
+}
+
+// ops.rs:309-316
+bool check_pair(int f, const char* name, const char* ln, size_t l, const char* rn, size_t r,
+                fgfc_status* st) {
+  if (l != r) {
+    *st = fail(FGFC_ERR_LENGTH, "%s: %s is %zu bytes but %s is %zu bytes", name, ln, l, rn, r);
+    return false;
+  }
+  return check_width(f, name, l, st);
+}
+
+bool mul_overflows(size_t a, size_t b, size_t* out) {
+  if (a && b > SIZE_MAX / a) return true;
+  *out = a * b;
+  return false;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- plans
+
+struct fgfc_plan {
+  int field;
+  size_t rows, cols;
+  std::vector<uint32_t> values;
+  int device;
+  uint32_t* dev;        // device tables, three orientations back to back
+  size_t mat_groups;    // groups per source in the matrix orientation
+  size_t off_mat, off_scat, off_gath;  // word offsets into `dev`
+  size_t scat_groups;
+};
+
+namespace {
+
+// Coefficient source for a lowered matrix call: either raw host values
+// (term-major, k x m) or device tables of a plan.
+struct CoeffSrc {
+  const uint32_t* host = nullptr;  // term-major k x m
+  const uint32_t* dev = nullptr;   // compact tables [(t*E+p)*gstride + g][32]
+  size_t gstride = 0;
+};
+
+std::mutex g_launch_mu;
+
+fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows,
+                       size_t m, const CoeffSrc& cs, size_t len, bool overwrite,
+                       cudaStream_t stream, const char* name) {
+  if (m == 0 || len == 0) return ok();
+  if (k == 0) {
+    if (overwrite) {
+      cudaError_t e = launch_zero_rows(rows, static_cast<int>(m), len, stream);
+      if (e != cudaSuccess) return cuda_fail(e, name);
+    }
+    return ok();
+  }
+  const int E = field_bytes(field);
+  const int R = 4 / E;
+  const size_t gtot = (m + R - 1) / R;
+  const bool inl = cs.dev == nullptr;
+  const size_t slot_cap = inl ? kInlineSlots : kMaxSlots;
+  size_t gp = std::min<size_t>(gtot, 4);
+  while (gp > 1 && static_cast<size_t>(E) * gp > slot_cap) --gp;
+  size_t kc = std::min<size_t>(k, slot_cap / (E * gp));
+  kc = std::min<size_t>(kc, kMaxSrc);
+  if (kc == 0) return fail(FGFC_ERR_LIMIT, "%s: internal tiling failed", name);
+
+  // Alignment class shared by every pointer of the call.
+  uintptr_t al = reinterpret_cast<uintptr_t>(srcs[0]) & 15;
+  bool same = true;
+  for (size_t t = 0; t < k; ++t) same &= (reinterpret_cast<uintptr_t>(srcs[t]) & 15) == al;
+  for (size_t j = 0; j < m; ++j) same &= (reinterpret_cast<uintptr_t>(rows[j]) & 15) == al;
+  same &= (al % E) == 0;
+  uint64_t head = len, nvec = 0;
+  if (same) {
+    head = std::min<uint64_t>((16 - al) & 15, len);
+    nvec = (len - head) / 16;
+  }
+
+  static thread_local MatrixLaunch a;  // large (inline tables): keep off the stack
+  for (size_t g0 = 0; g0 < gtot; g0 += gp) {
+    const size_t G = std::min(gp, gtot - g0);
+    const size_t r0 = g0 * R;
+    const size_t nr = std::min(m - r0, G * R);
+    for (size_t t0 = 0; t0 < k; t0 += kc) {
+      const size_t kk = std::min(kc, k - t0);
+      a.len = len;
+      a.head = head;
+      a.nvec = nvec;
+      a.k = static_cast<uint32_t>(kk);
+      a.nrows = static_cast<uint32_t>(nr);
+      for (size_t t = 0; t < kk; ++t) a.src[t] = srcs[t0 + t];
+      for (size_t j = 0; j < nr; ++j) a.dst[j] = rows[r0 + j];
+      if (inl) {
+        build_compact_tables(field, cs.host, m, t0, kk, g0, G, a.inline_tab);
+        a.tables = nullptr;
+        a.gstride = static_cast<uint32_t>(G);
+        a.g0 = 0;
+      } else {
+        a.tables = cs.dev + t0 * E * cs.gstride * kCompactWords;
+        a.gstride = static_cast<uint32_t>(cs.gstride);
+        a.g0 = static_cast<uint32_t>(g0);
+      }
+      cudaError_t e;
+      {
+        std::lock_guard<std::mutex> lk(g_launch_mu);
+        e = launch_matrix(field, static_cast<int>(G), overwrite && t0 == 0, a, stream);
+      }
+      if (e != cudaSuccess) return cuda_fail(e, name);
+    }
+  }
+  return ok();
+}
+
+bool all_zero(const uint32_t* c, size_t n, uint32_t mask) {
+  for (size_t i = 0; i < n; ++i)
+    if (c[i] & mask) return false;
+  return true;
+}
+
+fgfc_status upload_plan_tables(fgfc_plan* p) {
+  const int E = field_bytes(p->field);
+  const int R = 4 / E;
+  const size_t len = p->values.size();
+  // matrix orientation: rows = sources, cols = destination rows
+  p->mat_groups = p->cols ? (p->cols + R - 1) / R : 0;
+  const size_t n_mat = p->rows * E * p->mat_groups * kCompactWords;
+  p->scat_groups = len ? (len + R - 1) / R : 0;
+  const size_t n_scat = E * p->scat_groups * kCompactWords;
+  const size_t n_gath = len * E * kCompactWords;
+  std::vector<uint32_t> host(n_mat + n_scat + n_gath + 1, 0);
+  p->off_mat = 0;
+  p->off_scat = n_mat;
+  p->off_gath = n_mat + n_scat;
+  if (n_mat) build_compact_tables(p->field, p->values.data(), p->cols, 0, p->rows, 0, p->mat_groups,
+                                  host.data() + p->off_mat);
+  if (n_scat) build_compact_tables(p->field, p->values.data(), len, 0, 1, 0, p->scat_groups,
+                                   host.data() + p->off_scat);
+  if (n_gath) {
+    // gather orientation: source i has the single coefficient values[i]
+    build_compact_tables(p->field, p->values.data(), 1, 0, len, 0, 1, host.data() + p->off_gath);
+  }
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e != cudaSuccess) return cuda_fail(e, "Plan::matrix");
+  e = cudaMalloc(&p->dev, host.size() * sizeof(uint32_t));
+  if (e != cudaSuccess) return fail(FGFC_ERR_NOMEM, "Plan::matrix: device allocation failed: %s",
+                                    cudaGetErrorString(e));
+  e = cudaMemcpy(p->dev, host.data(), host.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "Plan::matrix");
+  return ok();
+}
+
+CoeffSrc plan_mat(const fgfc_plan* p) {
+  CoeffSrc c;
+  c.dev = p->dev + p->off_mat;
+  c.gstride = p->mat_groups;
+  return c;
+}
+CoeffSrc plan_scat(const fgfc_plan* p) {
+  CoeffSrc c;
+  c.dev = p->dev + p->off_scat;
+  c.gstride = p->scat_groups;
+  return c;
+}
+CoeffSrc plan_gath(const fgfc_plan* p) {
+  CoeffSrc c;
+  c.dev = p->dev + p->off_gath;
+  c.gstride = 1;
+  return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fgfc_last_error(void) { return t_err.c_str(); }
+const char* fgfc_version(void) { return "fgf-cuda 0.1.0 (sm_100a; mirrors fgf 0.4.0 ops)"; }
+
+void fgfc_limits(size_t* max_sources, size_t* max_rows) {
+  if (max_sources) *max_sources = SIZE_MAX;
+  if (max_rows) *max_rows = SIZE_MAX;
+}
+
+size_t fgfc_field_bytes(fgfc_field field) { return valid_field(field) ? field_bytes(field) : 0; }
+
+fgfc_status fgfc_plan_create(fgfc_field field, size_t rows, size_t cols, const uint32_t* coeffs,
+                             fgfc_plan** out) {
+  if (!out || !valid_field(field)) return fail(FGFC_ERR_ARG, "Plan::matrix: invalid argument");
+  *out = nullptr;
+  size_t n;
+  if (mul_overflows(rows, cols, &n)) return fail(FGFC_ERR_OVERFLOW, "Plan::matrix: dimensions overflow");
+  if (n && !coeffs) return fail(FGFC_ERR_ARG, "Plan::matrix: null coefficients");
+  fgfc_plan* p = new fgfc_plan();
+  p->field = field;
+  p->rows = rows;
+  p->cols = cols;
+  p->values.assign(coeffs, coeffs + n);
+  for (auto& v : p->values) v &= field_mask(field);
+  p->dev = nullptr;
+  fgfc_status st = upload_plan_tables(p);
+  if (st != FGFC_OK) {
+    fgfc_plan_destroy(p);
+    return st;
+  }
+  *out = p;
+  return ok();
+}
+
+fgfc_status fgfc_coeff_create(fgfc_field field, uint32_t coeff, fgfc_plan** out) {
+  return fgfc_plan_create(field, 1, 1, &coeff, out);
+}
+
+void fgfc_plan_destroy(fgfc_plan* plan) {
+  if (!plan) return;
+  if (plan->dev) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != plan->device) cudaSetDevice(plan->device);
+    cudaFree(plan->dev);
+    if (cur != plan->device) cudaSetDevice(cur);
+  }
+  delete plan;
+}
+
+fgfc_status fgfc_plan_dimensions(const fgfc_plan* plan, size_t* rows, size_t* cols) {
+  if (!plan) return fail(FGFC_ERR_ARG, "Plan: null plan");
+  if (rows) *rows = plan->rows;
+  if (cols) *cols = plan->cols;
+  return ok();
+}
+
+size_t fgfc_plan_len(const fgfc_plan* plan) { return plan ? plan->values.size() : 0; }
+
+fgfc_field fgfc_plan_field(const fgfc_plan* plan) {
+  return plan ? static_cast<fgfc_field>(plan->field) : FGFC_GF8B;
+}
+
+fgfc_status fgfc_plan_values(const fgfc_plan* plan, uint32_t* out) {
+  if (!plan || (!out && !plan->values.empty())) return fail(FGFC_ERR_ARG, "Plan: null argument");
+  std::copy(plan->values.begin(), plan->values.end(), out);
+  return ok();
+}
+
+fgfc_status fgfc_plan_get_at(const fgfc_plan* plan, size_t row, size_t col, uint32_t* out) {
+  if (!plan || !out) return fail(FGFC_ERR_ARG, "Plan: null argument");
+  if (row >= plan->rows || col >= plan->cols) return fail(FGFC_ERR_ARG, "Plan::get_at: out of bounds");
+  *out = plan->values[row * plan->cols + col];
+  return ok();
+}
+
+// ---------------------------------------------------------------- single row
+
+fgfc_status fgfc_add_assign(fgfc_field field, uint8_t* dst, size_t dst_len, const uint8_t* src,
+                            size_t src_len, fgfc_stream stream) {
+  fgfc_status st;
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "add_assign: unknown field");
+  if (!check_pair(field, "add_assign", "dst", dst_len, "src", src_len, &st)) return st;
+  cudaError_t e = launch_xor(dst, src, dst_len, stream);
+  return e == cudaSuccess ? ok() : cuda_fail(e, "add_assign");
+}
+
+static fgfc_status mul_add_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
+                                uint32_t coeff, const fgfc_plan* plan, const uint8_t* src,
+                                size_t src_len, cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_pair(field, name, "dst", dst_len, "src", src_len, &st)) return st;
+  coeff &= field_mask(field);
+  if (coeff == 0) return ok();
+  if (coeff == 1) {
+    cudaError_t e = launch_xor(dst, src, dst_len, stream);
+    return e == cudaSuccess ? ok() : cuda_fail(e, name);
+  }
+  uint8_t* rows[1] = {dst};
+  const uint8_t* srcs[1] = {src};
+  CoeffSrc cs;
+  if (plan) {
+    cs = plan_mat(plan);
+  } else {
+    cs.host = &coeff;
+  }
+  return run_matrix(field, srcs, 1, rows, 1, cs, dst_len, false, stream, name);
+}
+
+fgfc_status fgfc_mul_add(fgfc_field field, uint8_t* dst, size_t dst_len, uint32_t coeff,
+                         const uint8_t* src, size_t src_len, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add: unknown field");
+  return mul_add_impl(field, "mul_add", dst, dst_len, coeff, nullptr, src, src_len, stream);
+}
+
+static bool single_coeff(const fgfc_plan* p, const char* name, fgfc_status* st) {
+  if (!p) {
+    *st = fail(FGFC_ERR_ARG, "%s: null coefficient", name);
+    return false;
+  }
+  if (p->values.size() != 1) {
+    *st = fail(FGFC_ERR_ARG, "%s: a prepared coefficient holds exactly one value, this plan holds %zu",
+               name, p->values.size());
+    return false;
+  }
+  return true;
+}
+
+fgfc_status fgfc_mul_add_with(uint8_t* dst, size_t dst_len, const fgfc_plan* coeff,
+                              const uint8_t* src, size_t src_len, fgfc_stream stream) {
+  fgfc_status st;
+  if (!single_coeff(coeff, "mul_add_with", &st)) return st;
+  return mul_add_impl(coeff->field, "mul_add_with", dst, dst_len, coeff->values[0], coeff, src,
+                      src_len, stream);
+}
+
+static fgfc_status mul_into_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
+                                 uint32_t coeff, const fgfc_plan* plan, const uint8_t* src,
+                                 size_t src_len, cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_pair(field, name, "dst", dst_len, "src", src_len, &st)) return st;
+  coeff &= field_mask(field);
+  if (dst_len == 0) return ok();
+  if (coeff == 0) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, dst_len, stream);
+    return e == cudaSuccess ? ok() : cuda_fail(e, name);
+  }
+  if (coeff == 1) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, dst_len, cudaMemcpyDeviceToDevice, stream);
+    return e == cudaSuccess ? ok() : cuda_fail(e, name);
+  }
+  uint8_t* rows[1] = {dst};
+  const uint8_t* srcs[1] = {src};
+  CoeffSrc cs;
+  if (plan) {
+    cs = plan_mat(plan);
+  } else {
+    cs.host = &coeff;
+  }
+  return run_matrix(field, srcs, 1, rows, 1, cs, dst_len, true, stream, name);
+}
+
+fgfc_status fgfc_mul_into(fgfc_field field, uint8_t* dst, size_t dst_len, uint32_t coeff,
+                          const uint8_t* src, size_t src_len, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_into: unknown field");
+  return mul_into_impl(field, "mul_into", dst, dst_len, coeff, nullptr, src, src_len, stream);
+}
+
+fgfc_status fgfc_mul_into_with(uint8_t* dst, size_t dst_len, const fgfc_plan* coeff,
+                               const uint8_t* src, size_t src_len, fgfc_stream stream) {
+  fgfc_status st;
+  if (!single_coeff(coeff, "mul_into_with", &st)) return st;
+  return mul_into_impl(coeff->field, "mul_into_with", dst, dst_len, coeff->values[0], coeff, src,
+                       src_len, stream);
+}
+
+static fgfc_status mul_assign_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
+                                   uint32_t coeff, const fgfc_plan* plan, cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_width(field, name, dst_len, &st)) return st;
+  coeff &= field_mask(field);
+  if (coeff == 1 || dst_len == 0) return ok();
+  if (coeff == 0) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, dst_len, stream);
+    return e == cudaSuccess ? ok() : cuda_fail(e, name);
+  }
+  uint8_t* rows[1] = {dst};
+  const uint8_t* srcs[1] = {dst};  // in place: every byte is read before it is written, by one thread
+  CoeffSrc cs;
+  if (plan) {
+    cs = plan_mat(plan);
+  } else {
+    cs.host = &coeff;
+  }
+  return run_matrix(field, srcs, 1, rows, 1, cs, dst_len, true, stream, name);
+}
+
+fgfc_status fgfc_mul_assign(fgfc_field field, uint8_t* dst, size_t dst_len, uint32_t coeff,
+                            fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_assign: unknown field");
+  return mul_assign_impl(field, "mul_assign", dst, dst_len, coeff, nullptr, stream);
+}
+
+fgfc_status fgfc_mul_assign_with(uint8_t* dst, size_t dst_len, const fgfc_plan* coeff,
+                                 fgfc_stream stream) {
+  fgfc_status st;
+  if (!single_coeff(coeff, "mul_assign_with", &st)) return st;
+  return mul_assign_impl(coeff->field, "mul_assign_with", dst, dst_len, coeff->values[0], coeff,
+                         stream);
+}
+
+fgfc_status fgfc_mul_elementwise(fgfc_field field, uint8_t* dst, size_t dst_len, const uint8_t* a,
+                                 size_t a_len, const uint8_t* b, size_t b_len, fgfc_stream stream) {
+  fgfc_status st;
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_elementwise: unknown field");
+  if (!check_pair(field, "mul_elementwise", "dst", dst_len, "a", a_len, &st)) return st;
+  if (!check_pair(field, "mul_elementwise", "dst", dst_len, "b", b_len, &st)) return st;
+  cudaError_t e = launch_elementwise(field, dst, a, b, dst_len, stream);
+  return e == cudaSuccess ? ok() : cuda_fail(e, "mul_elementwise");
+}
+
+// ---------------------------------------------------------------- scatter / gather
+
+static fgfc_status scatter_impl(int field, const char* name, const char* count_word, uint8_t* rows,
+                                size_t rows_len, size_t row_len, const uint32_t* coeffs, size_t n,
+                                const fgfc_plan* plan, const uint8_t* src, size_t src_len,
+                                cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_pair(field, name, "row_len", row_len, "src", src_len, &st)) return st;
+  size_t used;
+  if (mul_overflows(n, row_len, &used)) return fail(FGFC_ERR_OVERFLOW, "%s: row geometry overflows", name);
+  if (rows_len < used)
+    return fail(FGFC_ERR_ROWS, "%s: rows is %zu bytes but %zu rows of %zu bytes need %zu", name,
+                rows_len, n, row_len, used);
+  (void)count_word;
+  if (all_zero(coeffs, n, field_mask(field))) return ok();
+  std::vector<uint8_t*> rp(n);
+  for (size_t j = 0; j < n; ++j) rp[j] = rows + j * row_len;
+  const uint8_t* srcs[1] = {src};
+  CoeffSrc cs;
+  if (plan) {
+    cs = plan_scat(plan);
+  } else {
+    cs.host = coeffs;
+  }
+  return run_matrix(field, srcs, 1, rp.data(), n, cs, row_len, false, stream, name);
+}
+
+fgfc_status fgfc_mul_add_scatter(fgfc_field field, uint8_t* rows, size_t rows_len, size_t row_len,
+                                 const uint32_t* coeffs, size_t ncoeffs, const uint8_t* src,
+                                 size_t src_len, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add_scatter: unknown field");
+  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  for (auto& v : c) v &= field_mask(field);
+  return scatter_impl(field, "mul_add_scatter", "coefficients", rows, rows_len, row_len, c.data(),
+                      ncoeffs, nullptr, src, src_len, stream);
+}
+
+fgfc_status fgfc_mul_add_scatter_with(uint8_t* rows, size_t rows_len, size_t row_len,
+                                      const fgfc_plan* plan, const uint8_t* src, size_t src_len,
+                                      fgfc_stream stream) {
+  if (!plan) return fail(FGFC_ERR_ARG, "mul_add_scatter_with: null plan");
+  return scatter_impl(plan->field, "mul_add_scatter_with", "plan", rows, rows_len, row_len,
+                      plan->values.data(), plan->values.size(), plan, src, src_len, stream);
+}
+
+// Shared validation of gather / dot_product (raw and prepared forms).
+static bool check_sources(int field, const char* name, bool with_plan, size_t dst_len, size_t ncoeffs,
+                          const fgfc_slice* srcs, size_t nsrcs, fgfc_status* st) {
+  if (!check_width(field, name, dst_len, st)) return false;
+  if (ncoeffs != nsrcs) {
+    if (with_plan)
+      *st = fail(FGFC_ERR_COEFFS, "%s: plan has %zu coefficients but there are %zu sources", name,
+                 ncoeffs, nsrcs);
+    else
+      *st = fail(FGFC_ERR_COEFFS, "%s: %zu coefficients for %zu sources", name, ncoeffs, nsrcs);
+    return false;
+  }
+  if (nsrcs && !srcs) {
+    *st = fail(FGFC_ERR_ARG, "%s: null sources", name);
+    return false;
+  }
+  for (size_t i = 0; i < nsrcs; ++i) {
+    if (srcs[i].len != dst_len) {
+      // mul_add_gather (raw) names no index: ops.rs:542-550
+      if (!with_plan && std::strcmp(name, "mul_add_gather") == 0)
+        *st = fail(FGFC_ERR_SOURCE, "%s: source is %zu bytes, expected %zu", name, srcs[i].len, dst_len);
+      else
+        *st = fail(FGFC_ERR_SOURCE, "%s: source %zu is %zu bytes, expected %zu", name, i, srcs[i].len,
+                   dst_len);
+      return false;
+    }
+  }
+  return true;
+}
+
+static fgfc_status gather_impl(int field, const char* name, bool with_plan, uint8_t* dst,
+                               size_t dst_len, const uint32_t* coeffs, size_t ncoeffs,
+                               const fgfc_plan* plan, const fgfc_slice* srcs, size_t nsrcs,
+                               bool overwrite, cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_sources(field, name, with_plan, dst_len, ncoeffs, srcs, nsrcs, &st)) return st;
+  const bool zero = nsrcs == 0 || all_zero(coeffs, ncoeffs, field_mask(field));
+  if (zero) {
+    if (overwrite && dst_len) {
+      cudaError_t e = cudaMemsetAsync(dst, 0, dst_len, stream);
+      if (e != cudaSuccess) return cuda_fail(e, name);
+    }
+    return ok();
+  }
+  if (overwrite && nsrcs == 1)  // ops.rs:619-622 / 654-658: one source is mul_into
+    return mul_into_impl(field, with_plan ? "mul_into_with" : "mul_into", dst, dst_len, coeffs[0],
+                         plan, srcs[0].ptr, srcs[0].len, stream);
+  std::vector<const uint8_t*> sp(nsrcs);
+  for (size_t i = 0; i < nsrcs; ++i) sp[i] = srcs[i].ptr;
+  uint8_t* rows[1] = {dst};
+  CoeffSrc cs;
+  if (plan) {
+    cs = plan_gath(plan);
+  } else {
+    cs.host = coeffs;  // k x 1, term-major
+  }
+  return run_matrix(field, sp.data(), nsrcs, rows, 1, cs, dst_len, overwrite, stream, name);
+}
+
+fgfc_status fgfc_mul_add_gather(fgfc_field field, uint8_t* dst, size_t dst_len,
+                                const uint32_t* coeffs, size_t ncoeffs, const fgfc_slice* srcs,
+                                size_t nsrcs, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add_gather: unknown field");
+  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  for (auto& v : c) v &= field_mask(field);
+  return gather_impl(field, "mul_add_gather", false, dst, dst_len, c.data(), ncoeffs, nullptr, srcs,
+                     nsrcs, false, stream);
+}
+
+fgfc_status fgfc_mul_add_gather_with(uint8_t* dst, size_t dst_len, const fgfc_plan* plan,
+                                     const fgfc_slice* srcs, size_t nsrcs, fgfc_stream stream) {
+  if (!plan) return fail(FGFC_ERR_ARG, "mul_add_gather_with: null plan");
+  return gather_impl(plan->field, "mul_add_gather_with", true, dst, dst_len, plan->values.data(),
+                     plan->values.size(), plan, srcs, nsrcs, false, stream);
+}
+
+fgfc_status fgfc_dot_product(fgfc_field field, uint8_t* dst, size_t dst_len,
+                             const uint32_t* coeffs, size_t ncoeffs, const fgfc_slice* srcs,
+                             size_t nsrcs, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "dot_product: unknown field");
+  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  for (auto& v : c) v &= field_mask(field);
+  return gather_impl(field, "dot_product", false, dst, dst_len, c.data(), ncoeffs, nullptr, srcs, nsrcs,
+                     true, stream);
+}
+
+fgfc_status fgfc_dot_product_with(uint8_t* dst, size_t dst_len, const fgfc_plan* plan,
+                                  const fgfc_slice* srcs, size_t nsrcs, fgfc_stream stream) {
+  if (!plan) return fail(FGFC_ERR_ARG, "dot_product_with: null plan");
+  // A single-source prepared dot product is mul_into_with on plan entry 0,
+  // whose device tables are the gather orientation's first slot.
+  return gather_impl(plan->field, "dot_product_with", true, dst, dst_len, plan->values.data(),
+                     plan->values.size(), plan, srcs, nsrcs, true, stream);
+}
+
+// ---------------------------------------------------------------- matrices
+
+static fgfc_status matrix_terms_impl(int field, const char* name, bool overwrite, uint8_t* rows,
+                                     size_t rows_len, size_t row_len, size_t nrows,
+                                     const fgfc_term* terms, size_t nterms, cudaStream_t stream) {
+  fgfc_status st;
+  if (!check_width(field, name, row_len, &st)) return st;
+  size_t used;
+  if (mul_overflows(nrows, row_len, &used)) return fail(FGFC_ERR_OVERFLOW, "%s: row geometry overflows", name);
+  if (rows_len < used)
+    return fail(FGFC_ERR_ROWS, "%s: rows is %zu bytes but %zu rows of %zu bytes need %zu", name,
+                rows_len, nrows, row_len, used);
+  if (nterms && !terms) return fail(FGFC_ERR_ARG, "%s: null terms", name);
+  for (size_t t = 0; t < nterms; ++t) {
+    if (terms[t].ncoeffs != nrows)
+      return fail(FGFC_ERR_COEFFS, "%s: term supplies %zu coefficients for %zu rows", name,
+                  terms[t].ncoeffs, nrows);
+    if (terms[t].src_len != row_len)
+      return fail(FGFC_ERR_SOURCE, "%s: source is %zu bytes, expected %zu", name, terms[t].src_len,
+                  row_len);
+  }
+  if (nrows == 0) return ok();
+  if (nterms == 0) {
+    if (overwrite && used) {
+      cudaError_t e = cudaMemsetAsync(rows, 0, used, stream);
+      if (e != cudaSuccess) return cuda_fail(e, name);
+    }
+    return ok();
+  }
+  std::vector<uint32_t> coeffs(nterms * nrows);
+  std::vector<const uint8_t*> sp(nterms);
+  for (size_t t = 0; t < nterms; ++t) {
+    sp[t] = terms[t].src;
+    for (size_t j = 0; j < nrows; ++j) coeffs[t * nrows + j] = terms[t].coeffs[j] & field_mask(field);
+  }
+  std::vector<uint8_t*> rp(nrows);
+  for (size_t j = 0; j < nrows; ++j) rp[j] = rows + j * row_len;
+  CoeffSrc cs;
+  cs.host = coeffs.data();
+  return run_matrix(field, sp.data(), nterms, rp.data(), nrows, cs, row_len, overwrite, stream, name);
+}
+
+fgfc_status fgfc_mul_add_matrix(fgfc_field field, uint8_t* rows, size_t rows_len, size_t row_len,
+                                size_t nrows, const fgfc_term* terms, size_t nterms,
+                                fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add_matrix: unknown field");
+  return matrix_terms_impl(field, "mul_add_matrix", false, rows, rows_len, row_len, nrows, terms,
+                           nterms, stream);
+}
+
+fgfc_status fgfc_dot_product_matrix(fgfc_field field, uint8_t* rows, size_t rows_len,
+                                    size_t row_len, size_t nrows, const fgfc_term* terms,
+                                    size_t nterms, fgfc_stream stream) {
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "dot_product_matrix: unknown field");
+  return matrix_terms_impl(field, "dot_product_matrix", true, rows, rows_len, row_len, nrows, terms,
+                           nterms, stream);
+}
+
+static fgfc_status matrix_plan_impl(const char* name, bool overwrite, uint8_t* rows, size_t rows_len,
+                                    size_t row_len, size_t nrows, const fgfc_plan* plan,
+                                    const fgfc_slice* srcs, size_t nsrcs, cudaStream_t stream) {
+  fgfc_status st;
+  if (!plan) return fail(FGFC_ERR_ARG, "%s: null plan", name);
+  const int field = plan->field;
+  if (!check_width(field, name, row_len, &st)) return st;
+  size_t used;
+  if (mul_overflows(nrows, row_len, &used)) return fail(FGFC_ERR_OVERFLOW, "%s: row geometry overflows", name);
+  if (rows_len < used)
+    return fail(FGFC_ERR_ROWS, "%s: rows is %zu bytes but %zu rows of %zu bytes need %zu", name,
+                rows_len, nrows, row_len, used);
+  if (plan->rows != nsrcs || plan->cols != nrows)
+    return fail(FGFC_ERR_PLAN_DIMS, "%s: plan dimensions do not match (sources, rows)", name);
+  if (nsrcs && !srcs) return fail(FGFC_ERR_ARG, "%s: null sources", name);
+  for (size_t i = 0; i < nsrcs; ++i)
+    if (srcs[i].len != row_len)
+      return fail(FGFC_ERR_SOURCE, "%s: source %zu is %zu bytes, expected %zu", name, i, srcs[i].len,
+                  row_len);
+  if (nrows == 0) return ok();
+  if (nsrcs == 0) {
+    if (overwrite && used) {
+      cudaError_t e = cudaMemsetAsync(rows, 0, used, stream);
+      if (e != cudaSuccess) return cuda_fail(e, name);
+    }
+    return ok();
+  }
+  std::vector<const uint8_t*> sp(nsrcs);
+  for (size_t i = 0; i < nsrcs; ++i) sp[i] = srcs[i].ptr;
+  std::vector<uint8_t*> rp(nrows);
+  for (size_t j = 0; j < nrows; ++j) rp[j] = rows + j * row_len;
+  return run_matrix(field, sp.data(), nsrcs, rp.data(), nrows, plan_mat(plan), row_len, overwrite,
+                    stream, name);
+}
+
+fgfc_status fgfc_mul_add_matrix_with(uint8_t* rows, size_t rows_len, size_t row_len, size_t nrows,
+                                     const fgfc_plan* plan, const fgfc_slice* srcs, size_t nsrcs,
+                                     fgfc_stream stream) {
+  return matrix_plan_impl("mul_add_matrix_with", false, rows, rows_len, row_len, nrows, plan, srcs,
+                          nsrcs, stream);
+}
+
+fgfc_status fgfc_dot_product_matrix_with(uint8_t* rows, size_t rows_len, size_t row_len,
+                                         size_t nrows, const fgfc_plan* plan,
+                                         const fgfc_slice* srcs, size_t nsrcs,
+                                         fgfc_stream stream) {
+  return matrix_plan_impl("dot_product_matrix_with", true, rows, rows_len, row_len, nrows, plan, srcs,
+                          nsrcs, stream);
+}
+
+// ops.rs:887-941
+static bool check_scattered_rows(int field, const char* name, size_t dst_len, size_t row_len,
+                                 const size_t* row_starts, size_t nrows, fgfc_status* st) {
+  if (!check_width(field, name, row_len, st)) return false;
+  if (nrows && !row_starts) {
+    *st = fail(FGFC_ERR_ARG, "%s: null row_starts", name);
+    return false;
+  }
+  for (size_t j = 0; j < nrows; ++j) {
+    const size_t start = row_starts[j];
+    if (start > SIZE_MAX - row_len) {
+      *st = fail(FGFC_ERR_OVERFLOW, "%s: row offset + length overflows", name);
+      return false;
+    }
+    const size_t end = start + row_len;
+    if (end > dst_len) {
+      *st = fail(FGFC_ERR_BOUNDS, "%s: row %zu spans %zu..%zu but dst is %zu bytes", name, j, start, end,
+                 dst_len);
+      return false;
+    }
+    if (start % field_bytes(field) != 0) {
+      *st = fail(FGFC_ERR_ALIGN, "%s: row %zu offset %zu is not a whole number of %s elements", name, j,
+                 start, field_name(field));
+      return false;
+    }
+  }
+  for (size_t a = 0; a < nrows; ++a)
+    for (size_t b = a + 1; b < nrows; ++b) {
+      const size_t sa = row_starts[a], sb = row_starts[b];
+      const size_t lo = std::min(sa, sb), hi = std::max(sa, sb);
+      if (hi - lo < row_len) {
+        *st = fail(FGFC_ERR_OVERLAP, "%s: rows at %zu and %zu overlap for %zu-byte rows", name, sa, sb,
+                   row_len);
+        return false;
+      }
+    }
+  return true;
+}
+
+fgfc_status fgfc_mul_add_matrix_scattered(fgfc_field field, uint8_t* dst, size_t dst_len,
+                                          size_t row_len, const size_t* row_starts, size_t nrows,
+                                          const fgfc_term* terms, size_t nterms,
+                                          fgfc_stream stream) {
+  const char* name = "mul_add_matrix_scattered";
+  fgfc_status st;
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "%s: unknown field", name);
+  if (!check_scattered_rows(field, name, dst_len, row_len, row_starts, nrows, &st)) return st;
+  if (nterms && !terms) return fail(FGFC_ERR_ARG, "%s: null terms", name);
+  for (size_t t = 0; t < nterms; ++t) {
+    if (terms[t].ncoeffs != nrows)
+      return fail(FGFC_ERR_COEFFS, "%s: term supplies %zu coefficients for %zu rows", name,
+                  terms[t].ncoeffs, nrows);
+    if (terms[t].src_len != row_len)
+      return fail(FGFC_ERR_SOURCE, "%s: source is %zu bytes, expected %zu", name, terms[t].src_len,
+                  row_len);
+  }
+  if (nrows == 0 || nterms == 0) return ok();
+  std::vector<uint32_t> coeffs(nterms * nrows);
+  std::vector<const uint8_t*> sp(nterms);
+  for (size_t t = 0; t < nterms; ++t) {
+    sp[t] = terms[t].src;
+    for (size_t j = 0; j < nrows; ++j) coeffs[t * nrows + j] = terms[t].coeffs[j] & field_mask(field);
+  }
+  std::vector<uint8_t*> rp(nrows);
+  for (size_t j = 0; j < nrows; ++j) rp[j] = dst + row_starts[j];
+  CoeffSrc cs;
+  cs.host = coeffs.data();
+  return run_matrix(field, sp.data(), nterms, rp.data(), nrows, cs, row_len, false, stream, name);
+}
+
+fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t* dst, size_t dst_len, size_t row_len,
+                                               const size_t* row_starts, size_t nrows,
+                                               const fgfc_plan* plan, const fgfc_slice* srcs,
+                                               size_t nsrcs, fgfc_stream stream) {
+  const char* name = "mul_add_matrix_scattered_with";
+  fgfc_status st;
+  if (!plan) return fail(FGFC_ERR_ARG, "%s: null plan", name);
+  if (!check_scattered_rows(plan->field, name, dst_len, row_len, row_starts, nrows, &st)) return st;
+  if (plan->rows != nsrcs || plan->cols != nrows)
+    return fail(FGFC_ERR_PLAN_DIMS, "%s: plan dimensions do not match (sources, rows)", name);
+  if (nsrcs && !srcs) return fail(FGFC_ERR_ARG, "%s: null sources", name);
+  for (size_t i = 0; i < nsrcs; ++i)
+    if (srcs[i].len != row_len)
+      return fail(FGFC_ERR_SOURCE, "%s: source %zu is %zu bytes, expected %zu", name, i, srcs[i].len,
+                  row_len);
+  if (nrows == 0 || nsrcs == 0) return ok();
+  std::vector<const uint8_t*> sp(nsrcs);
+  for (size_t i = 0; i < nsrcs; ++i) sp[i] = srcs[i].ptr;
+  std::vector<uint8_t*> rp(nrows);
+  for (size_t j = 0; j < nrows; ++j) rp[j] = dst + row_starts[j];
+  return run_matrix(plan->field, sp.data(), nsrcs, rp.data(), nrows, plan_mat(plan), row_len, false,
+                    stream, name);
+}
+
+}  // extern "C"

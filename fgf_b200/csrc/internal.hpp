@@ -1,0 +1,66 @@
+// internal.hpp -- shared declarations between the C ABI layer (api.cpp) and
+// the device code (kernels.cu) of libfgfcuda.so.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "gf_host.hpp"
+
+namespace fgfc {
+
+// Limits of one kernel launch. Calls with more sources or rows are split
+// into several launches by the host (exact: rows are independent, and
+// sources split into an overwrite launch followed by accumulate launches).
+constexpr int kMaxSrc = 64;
+constexpr int kMaxRows = 64;
+// One nibble table slot: 16 rows x 256 bytes. Each row holds 32 lane copies
+// of the lo-nibble word (bytes 0..127) and of the hi-nibble word (128..255),
+// so a warp's 32 lookups hit 32 distinct banks.
+constexpr int kSlotBytes = 4096;
+constexpr int kMaxSlots = 56;            // 224 KiB of tables per CTA
+constexpr int kInlineSlots = 48;         // tables carried in launch parameters
+constexpr int kCompactWords = 32;        // 16 lo + 16 hi words per slot
+
+// A compact table slot for (source t, source byte-plane p, row group g):
+// word[n] (n < 16) = products of the lo nibble value n, word[16 + n] =
+// products of (n << 4); byte q of each word is output byte (q % E) of row
+// (g * R + q / E), R = 4 / E rows per group.
+
+struct MatrixLaunch {
+  uint64_t len;            // bytes per row processed by this launch
+  uint64_t head;           // bytes handled by the scalar path before the vector body
+  uint64_t nvec;           // 16-byte vectors in the body
+  uint32_t k;              // sources
+  uint32_t nrows;          // rows written by this launch (<= groups * R)
+  uint32_t gstride;        // groups per (source, plane) in the compact table array
+  uint32_t g0;             // first group of this launch within that array
+  const uint32_t* tables;  // device compact tables, or nullptr for `inline_tab`
+  const uint8_t* src[kMaxSrc];
+  uint8_t* dst[kMaxRows];
+  uint32_t inline_tab[kInlineSlots * kCompactWords];
+};
+
+// Build compact tables for sources [t0, t0+k) and groups [g0, g0+G) of a
+// coefficient matrix (term-major: coeffs[t * m + j]). Output layout
+// [(t * E + p) * G + g][32].
+void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0, size_t k,
+                          size_t g0, size_t G, uint32_t* out);
+
+// Kernel entry (kernels.cu). `groups` = G for this launch; `overwrite`
+// selects dot-product (overwrite) or mul_add (accumulate) semantics.
+cudaError_t launch_matrix(int field, int groups, bool overwrite, const MatrixLaunch& a,
+                          cudaStream_t s);
+// Fill `n` rows of `len` bytes with zero.
+cudaError_t launch_zero_rows(uint8_t* const* rows, int n, uint64_t len, cudaStream_t s);
+// dst ^= src over `len` bytes.
+cudaError_t launch_xor(uint8_t* dst, const uint8_t* src, uint64_t len, cudaStream_t s);
+// Elementwise product dst[i] = a[i] * b[i].
+cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
+                               uint64_t len, cudaStream_t s);
+
+int sm_count();
+
+}  // namespace fgfc

@@ -1,0 +1,614 @@
+// kernels.cu -- sm_100a kernels of libfgfcuda.so.
+//
+// One kernel family computes every shape of the reference's `ops` AXPY
+// family (src/ops.rs:342-941): rows[j] (^)= XOR_t c[t][j] * src_t, with the
+// destination rows given as pointers (contiguous or scattered) and
+// overwrite (dot_product*) or accumulate (mul_add*) semantics.
+//
+// Arithmetic: multiplying a packed element by a fixed coefficient is linear
+// over its byte subfield, so every output byte is an XOR of products of
+// source bytes with constants (gf_host.hpp: coeff_byte_matrix). Products are
+// read from split-nibble tables in shared memory: per (source, source byte
+// plane, group of 4 output bytes) a 16-entry table for the low nibble and
+// one for the high nibble, each entry a 32-bit word carrying the products
+// for 4 output bytes at once (4 Gf8 rows, 2 Gf16 rows or 1 Gf32 row). Every
+// table row is replicated across the 32 banks so a warp's lookups never
+// conflict, and one PRMT forms each lookup address from the nibble, the
+// lane and the table slot. The destination tile stays in registers while all
+// sources are folded in, as the reference's blocked CPU kernels do
+// (src/kernel/x86/gf8.rs:2208-2315), and is written once.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "internal.hpp"
+
+namespace fgfc {
+
+extern __shared__ __align__(16) uint8_t g_smem[];
+
+namespace {
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
+  return __byte_perm(a, b, s);
+}
+
+__device__ __forceinline__ uint32_t lds_at(uint32_t off) {
+  return *reinterpret_cast<const uint32_t*>(g_smem + off);
+}
+
+__device__ __forceinline__ uint4 ldg16(const uint8_t* p) {
+  return __ldg(reinterpret_cast<const uint4*>(p));
+}
+
+// Copy compact tables for this launch into the replicated shared layout:
+// word index i of the shared area is slot (i >> 10), nibble row
+// ((i >> 6) & 15), half ((i >> 5) & 1), lane (i & 31).
+template <int E, int G>
+__device__ __forceinline__ void fill_tables(const MatrixLaunch& a) {
+  const uint32_t nwords = a.k * E * G * 1024u;
+  uint32_t* st = reinterpret_cast<uint32_t*>(g_smem);
+  for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) {
+    const uint32_t slot = i >> 10;                 // (t * E + p) * G + g
+    const uint32_t g = slot % G;
+    const uint32_t tp = slot / G;
+    const uint32_t word = ((i >> 5) & 1u) * 16u + ((i >> 6) & 15u);
+    const uint32_t src = (tp * a.gstride + a.g0 + g) * kCompactWords + word;
+    st[i] = a.tables ? __ldg(a.tables + src) : a.inline_tab[src];
+  }
+}
+
+// Per-source lookup context: the byte pattern that places each byte's slot
+// (low 4 bits) next to its nibble, and per plane the register supplying the
+// lane offset (byte 0) and the 64 KiB page of the slot (bytes 2..3).
+template <int E, int G>
+struct SrcCtx {
+  uint32_t pat;
+  uint32_t lr[E];
+  __device__ __forceinline__ SrcCtx(uint32_t t, uint32_t lane4) {
+    pat = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const uint32_t s = (t * E + (b % E)) * G;
+      pat |= (s & 15u) << (8 * b + 4);
+    }
+#pragma unroll
+    for (int p = 0; p < E; ++p) {
+      const uint32_t s = (t * E + p) * G;
+      lr[p] = lane4 | ((s >> 4) << 16);
+    }
+  }
+};
+
+// Fold the 4 source bytes of word `w` (whole elements) into the
+// accumulators of their elements: acc[g][e0 + b / E] for byte b.
+template <int E, int G, int NE>
+__device__ __forceinline__ void fold_word(uint32_t w, const SrcCtx<E, G>& c, uint32_t (&acc)[G][NE],
+                                          int e0) {
+  const uint32_t xl = (w & 0x0F0F0F0Fu) | c.pat;
+  const uint32_t xh = ((w >> 4) & 0x0F0F0F0Fu) | c.pat;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+    const uint32_t al = prmt(xl, c.lr[b % E], sel);
+    const uint32_t ah = prmt(xh, c.lr[b % E], sel);
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      acc[g][e0 + b / E] ^= lds_at(al + g * kSlotBytes) ^ lds_at(ah + g * kSlotBytes + 128);
+  }
+}
+
+// Assemble output word q (16-byte step: q < 4; scalar step: q = 0) of row
+// rr of group g from the element accumulators.
+template <int E, int G, int NE>
+__device__ __forceinline__ uint32_t out_word(const uint32_t (&acc)[G][NE], int g, int rr, int q) {
+  if (E == 1) {
+    const uint32_t a0 = acc[g][4 * q], a1 = acc[g][4 * q + 1], a2 = acc[g][4 * q + 2],
+                   a3 = acc[g][4 * q + 3];
+    const uint32_t s01 = (rr < 2) ? prmt(a0, a1, 0x5140u) : prmt(a0, a1, 0x7362u);
+    const uint32_t s23 = (rr < 2) ? prmt(a2, a3, 0x5140u) : prmt(a2, a3, 0x7362u);
+    return (rr & 1) ? prmt(s01, s23, 0x7632u) : prmt(s01, s23, 0x5410u);
+  } else if (E == 2) {
+    return prmt(acc[g][2 * q], acc[g][2 * q + 1], rr ? 0x7632u : 0x5410u);
+  } else {
+    return acc[g][q];
+  }
+}
+
+template <int E, int G, bool OVR>
+__global__ void __launch_bounds__(512, (16 / E) * G <= 16 ? 2 : 1)
+    matrix_vec_kernel(const __grid_constant__ MatrixLaunch a) {
+  constexpr int NE = 16 / E;  // elements per 16-byte step
+  constexpr int R = 4 / E;    // rows per group
+  fill_tables<E, G>(a);
+  __syncthreads();
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < a.nvec;
+       v += stride) {
+    const uint64_t off = a.head + v * 16u;
+    uint32_t acc[G][NE];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < NE; ++e) acc[g][e] = 0;
+    uint4 cur = ldg16(a.src[0] + off);
+    for (uint32_t t = 0; t < a.k; ++t) {
+      uint4 nxt = cur;
+      if (t + 1 < a.k) nxt = ldg16(a.src[t + 1] + off);
+      const SrcCtx<E, G> c(t, lane4);
+      fold_word<E, G, NE>(cur.x, c, acc, 0 * (4 / E));
+      fold_word<E, G, NE>(cur.y, c, acc, 1 * (4 / E));
+      fold_word<E, G, NE>(cur.z, c, acc, 2 * (4 / E));
+      fold_word<E, G, NE>(cur.w, c, acc, 3 * (4 / E));
+      cur = nxt;
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        const uint32_t row = g * R + rr;
+        if (row >= a.nrows) continue;
+        uint4 o;
+        o.x = out_word<E, G, NE>(acc, g, rr, 0);
+        o.y = out_word<E, G, NE>(acc, g, rr, 1);
+        o.z = out_word<E, G, NE>(acc, g, rr, 2);
+        o.w = out_word<E, G, NE>(acc, g, rr, 3);
+        uint4* dp = reinterpret_cast<uint4*>(a.dst[row] + off);
+        if (!OVR) {
+          const uint4 d = *dp;
+          o.x ^= d.x;
+          o.y ^= d.y;
+          o.z ^= d.z;
+          o.w ^= d.w;
+        }
+        *dp = o;
+      }
+  }
+}
+
+// Scalar path: 4-byte groups with byte loads and stores, for the unaligned
+// head and tail of the vector body and for buffers whose pointers do not
+// share an alignment. Ranges [r0s, r0e) and [r1s, r1e) of every row; each
+// range starts on an element boundary.
+struct ScalarRanges {
+  uint64_t r0s, r0e, r1s, r1e;
+};
+
+template <int E, int G, bool OVR>
+__global__ void __launch_bounds__(256) matrix_scalar_kernel(const __grid_constant__ MatrixLaunch a,
+                                                            ScalarRanges rg) {
+  constexpr int R = 4 / E;
+  fill_tables<E, G>(a);
+  __syncthreads();
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint64_t n0 = (rg.r0e - rg.r0s + 3) / 4, n1 = (rg.r1e - rg.r1s + 3) / 4;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n0 + n1;
+       i += stride) {
+    const uint64_t off = i < n0 ? rg.r0s + 4 * i : rg.r1s + 4 * (i - n0);
+    const uint64_t end = i < n0 ? rg.r0e : rg.r1e;
+    const int nb = static_cast<int>(end - off < 4 ? end - off : 4);
+    uint32_t acc[G][4 / E];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < 4 / E; ++e) acc[g][e] = 0;
+    for (uint32_t t = 0; t < a.k; ++t) {
+      const uint8_t* s = a.src[t] + off;
+      uint32_t w = 0;
+      for (int b = 0; b < nb; ++b) w |= static_cast<uint32_t>(s[b]) << (8 * b);
+      const SrcCtx<E, G> c(t, lane4);
+      fold_word<E, G, 4 / E>(w, c, acc, 0);
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        const uint32_t row = g * R + rr;
+        if (row >= a.nrows) continue;
+        uint32_t o;
+        if (E == 1) {
+          o = prmt(prmt(acc[g][0], acc[g][1], rr < 2 ? 0x5140u : 0x7362u),
+                   prmt(acc[g][2], acc[g][3], rr < 2 ? 0x5140u : 0x7362u),
+                   (rr & 1) ? 0x7632u : 0x5410u);
+        } else if (E == 2) {
+          o = prmt(acc[g][0], acc[g][1], rr ? 0x7632u : 0x5410u);
+        } else {
+          o = acc[g][0];
+        }
+        uint8_t* d = a.dst[row] + off;
+        for (int b = 0; b < nb; ++b) {
+          const uint8_t v = static_cast<uint8_t>(o >> (8 * b));
+          d[b] = OVR ? v : static_cast<uint8_t>(d[b] ^ v);
+        }
+      }
+  }
+}
+
+// ---------------------------------------------------------------- byte-table kernel
+//
+// Gf8 fields with at most 4 rows (one table group) and a compile-time number
+// of sources K: the RS(10,4) encode / reconstruct shape and the single-row
+// ops. Sources t < kByteSrc get a full 256-entry product table (one lookup
+// per source byte, 32 KiB with the 32 lane copies; two tables share each
+// 64 KiB page, at byte offsets 0 and 128 of every 256-byte row), the rest
+// keep split-nibble tables in 4 KiB slots after the three byte-table pages.
+// With K fixed every table address is a PRMT of the data byte plus an
+// immediate, and the next column's sources are prefetched into registers
+// while the current one is folded.
+constexpr int kByteSrc = 6;
+constexpr uint32_t kNibbleBase = 3u * 65536u;
+// Rows shorter than this (in 16-byte vectors) use the nibble kernel: the
+// byte tables cost about a microsecond per CTA to fill.
+constexpr uint64_t kFastMinVec = 1u << 18;  // 4 MiB
+
+template <int K>
+struct FastLayout {
+  static constexpr int NB = K < kByteSrc ? K : kByteSrc;  // byte-table sources
+  static constexpr int NN = K - NB;                       // nibble-table sources
+  static constexpr uint32_t smem = NN ? kNibbleBase + NN * kSlotBytes : ((NB + 1) / 2) * 65536u;
+};
+
+template <int K>
+__device__ __forceinline__ void fill_fast_tables(const MatrixLaunch& a) {
+  using L = FastLayout<K>;
+  uint32_t* st = reinterpret_cast<uint32_t*>(g_smem);
+  auto compact = [&](uint32_t t, uint32_t w) -> uint32_t {
+    const uint32_t i = t * a.gstride * kCompactWords + a.g0 * kCompactWords + w;
+    return a.tables ? __ldg(a.tables + i) : a.inline_tab[i];
+  };
+  // byte tables: word index = page * 16384 + x * 64 + half * 32 + lane
+  for (uint32_t i = threadIdx.x; i < L::NB * 8192u; i += blockDim.x) {
+    const uint32_t t = i >> 13, x = (i >> 5) & 255u, lane = i & 31u;
+    st[(t >> 1) * 16384u + x * 64u + (t & 1u) * 32u + lane] =
+        compact(t, x & 15u) ^ compact(t, 16u + (x >> 4));
+  }
+  // nibble slots for sources NB..K-1
+  for (uint32_t i = threadIdx.x; i < L::NN * 1024u; i += blockDim.x) {
+    const uint32_t s = i >> 10;
+    st[kNibbleBase / 4 + i] = compact(L::NB + s, ((i >> 5) & 1u) * 16u + ((i >> 6) & 15u));
+  }
+}
+
+template <int K, bool OVR, bool PREFETCH>
+__global__ void __launch_bounds__(512, 1) matrix_fast_kernel(const __grid_constant__ MatrixLaunch a) {
+  using L = FastLayout<K>;
+  fill_fast_tables<K>(a);
+  __syncthreads();
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  uint32_t lrp[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) lrp[p] = lane4 | (static_cast<uint32_t>(p) << 16);
+  const uint32_t lrn = lane4 | (3u << 16);  // nibble slots live in page 3
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  uint4 nxt[K];
+  if (PREFETCH && v < a.nvec) {
+#pragma unroll
+    for (int t = 0; t < K; ++t) nxt[t] = ldg16(a.src[t] + a.head + v * 16u);
+  }
+  for (; v < a.nvec; v += stride) {
+    const uint64_t off = a.head + v * 16u;
+    uint4 cur[K];
+#pragma unroll
+    for (int t = 0; t < K; ++t) cur[t] = PREFETCH ? nxt[t] : ldg16(a.src[t] + off);
+    if (PREFETCH && v + stride < a.nvec) {
+#pragma unroll
+      for (int t = 0; t < K; ++t) nxt[t] = ldg16(a.src[t] + off + stride * 16u);
+    }
+    uint32_t acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0;
+    // byte-table sources, in pairs sharing one page
+#pragma unroll
+    for (int t = 0; t < L::NB; t += 2) {
+      const uint32_t lr = lrp[t >> 1];
+      const uint32_t wa[4] = {cur[t].x, cur[t].y, cur[t].z, cur[t].w};
+      if (t + 1 < L::NB) {
+        const uint32_t wb[4] = {cur[t + 1].x, cur[t + 1].y, cur[t + 1].z, cur[t + 1].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+            acc[4 * q + b] ^= lds_at(prmt(wa[q], lr, sel)) ^ lds_at(prmt(wb[q], lr, sel) + 128u);
+          }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+            acc[4 * q + b] ^= lds_at(prmt(wa[q], lr, sel));
+          }
+      }
+    }
+    // nibble-table sources
+#pragma unroll
+    for (int i = 0; i < L::NN; ++i) {
+      const uint32_t pat = ((static_cast<uint32_t>(48 + i) & 15u) << 4) * 0x01010101u;
+      const uint32_t w4[4] = {cur[L::NB + i].x, cur[L::NB + i].y, cur[L::NB + i].z, cur[L::NB + i].w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t xl = (w4[q] & 0x0F0F0F0Fu) | pat;
+        const uint32_t xh = ((w4[q] >> 4) & 0x0F0F0F0Fu) | pat;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+          acc[4 * q + b] ^= lds_at(prmt(xl, lrn, sel)) ^ lds_at(prmt(xh, lrn, sel) + 128u);
+        }
+      }
+    }
+    // 4x4 byte transposes: acc[e] holds rows 0..3 of element e
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) {
+      if (rr >= static_cast<int>(a.nrows)) break;
+      uint4 o;
+      uint32_t* ow = &o.x;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t s01 = prmt(acc[4 * q], acc[4 * q + 1], rr < 2 ? 0x5140u : 0x7362u);
+        const uint32_t s23 = prmt(acc[4 * q + 2], acc[4 * q + 3], rr < 2 ? 0x5140u : 0x7362u);
+        ow[q] = prmt(s01, s23, (rr & 1) ? 0x7632u : 0x5410u);
+      }
+      uint4* dp = reinterpret_cast<uint4*>(a.dst[rr] + off);
+      if (!OVR) {
+        const uint4 dv = *dp;
+        o.x ^= dv.x;
+        o.y ^= dv.y;
+        o.z ^= dv.z;
+        o.w ^= dv.w;
+      }
+      *dp = o;
+    }
+  }
+}
+
+int g_sms = 0;
+
+template <int K, bool OVR>
+cudaError_t launch_fast_k(const MatrixLaunch& a, cudaStream_t s) {
+  constexpr bool PF = K <= 10;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR, PF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         FastLayout<K>::smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const uint64_t want = (a.nvec + 511) / 512;
+  const uint64_t cap = static_cast<uint64_t>(sm_count());
+  const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+  matrix_fast_kernel<K, OVR, PF><<<blocks, 512, FastLayout<K>::smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <bool OVR>
+cudaError_t launch_fast(const MatrixLaunch& a, cudaStream_t s) {
+  switch (a.k) {
+    case 1: return launch_fast_k<1, OVR>(a, s);
+    case 2: return launch_fast_k<2, OVR>(a, s);
+    case 3: return launch_fast_k<3, OVR>(a, s);
+    case 4: return launch_fast_k<4, OVR>(a, s);
+    case 5: return launch_fast_k<5, OVR>(a, s);
+    case 6: return launch_fast_k<6, OVR>(a, s);
+    case 7: return launch_fast_k<7, OVR>(a, s);
+    case 8: return launch_fast_k<8, OVR>(a, s);
+    case 9: return launch_fast_k<9, OVR>(a, s);
+    case 10: return launch_fast_k<10, OVR>(a, s);
+    case 11: return launch_fast_k<11, OVR>(a, s);
+    case 12: return launch_fast_k<12, OVR>(a, s);
+    case 13: return launch_fast_k<13, OVR>(a, s);
+    case 14: return launch_fast_k<14, OVR>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int E, int G, bool OVR>
+cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
+  static bool configured = false;
+  static int occ_vec = 1;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxSlots * kSlotBytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(matrix_scalar_kernel<E, G, OVR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSlots * kSlotBytes);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const size_t smem = static_cast<size_t>(a.k) * E * G * kSlotBytes;
+  const int sms = sm_count();
+  if (E == 1 && G == 1 && a.k <= 14 && a.nvec >= kFastMinVec) {
+    cudaError_t e = launch_fast<OVR>(a, s);
+    if (e != cudaSuccess) return e;
+  } else if (a.nvec) {
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, matrix_vec_kernel<E, G, OVR>,
+                                                                  512, smem);
+    if (e != cudaSuccess) return e;
+    occ_vec = occ > 0 ? occ : 1;
+    uint64_t want = (a.nvec + 511) / 512;
+    uint64_t cap = static_cast<uint64_t>(sms) * occ_vec;
+    const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+    matrix_vec_kernel<E, G, OVR><<<blocks, 512, smem, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  ScalarRanges rg;
+  rg.r0s = 0;
+  rg.r0e = a.head;
+  rg.r1s = a.head + a.nvec * 16;
+  rg.r1e = a.len;
+  const uint64_t ngroups = (rg.r0e - rg.r0s + 3) / 4 + (rg.r1e - rg.r1s + 3) / 4;
+  if (ngroups) {
+    uint64_t want = (ngroups + 255) / 256;
+    uint64_t cap = static_cast<uint64_t>(sms) * 2;
+    const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+    matrix_scalar_kernel<E, G, OVR><<<blocks, 256, smem, s>>>(a, rg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <int E, bool OVR>
+cudaError_t launch_e(int groups, const MatrixLaunch& a, cudaStream_t s) {
+  switch (groups) {
+    case 1: return launch_one<E, 1, OVR>(a, s);
+    case 2: return launch_one<E, 2, OVR>(a, s);
+    case 3: return launch_one<E, 3, OVR>(a, s);
+    case 4: return launch_one<E, 4, OVR>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ---------------------------------------------------------------- helpers
+
+__global__ void xor_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint64_t len,
+                           uint64_t head, uint64_t nvec) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (uint64_t v = tid; v < nvec; v += stride) {
+    uint4* d = reinterpret_cast<uint4*>(dst + head + 16 * v);
+    const uint4 x = ldg16(src + head + 16 * v);
+    uint4 y = *d;
+    y.x ^= x.x;
+    y.y ^= x.y;
+    y.z ^= x.z;
+    y.w ^= x.w;
+    *d = y;
+  }
+  const uint64_t tail0 = head + 16 * nvec;
+  for (uint64_t i = tid; i < head + (len - tail0); i += stride) {
+    const uint64_t o = i < head ? i : tail0 + (i - head);
+    dst[o] ^= src[o];
+  }
+}
+
+__constant__ uint8_t c_exp[2][512];
+__constant__ uint8_t c_log[2][256];
+bool g_const_ready = false;
+
+__device__ __forceinline__ uint8_t emul(const uint8_t* ex, const uint8_t* lg, uint8_t x, uint8_t y) {
+  return (x && y) ? ex[lg[x] + lg[y]] : 0;
+}
+
+template <int F>
+__global__ void elementwise_kernel(uint8_t* dst, const uint8_t* a, const uint8_t* b, uint64_t nelem) {
+  __shared__ uint8_t ex[512];
+  __shared__ uint8_t lg[256];
+  constexpr int sel = (F == kGf8D) ? 1 : 0;
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) ex[i] = c_exp[sel][i];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lg[i] = c_log[sel][i];
+  __syncthreads();
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem;
+       i += stride) {
+    if (F == kGf8B || F == kGf8D) {
+      dst[i] = emul(ex, lg, a[i], b[i]);
+    } else if (F == kGf16) {
+      const uint8_t x0 = a[2 * i], x1 = a[2 * i + 1], y0 = b[2 * i], y1 = b[2 * i + 1];
+      const uint8_t ac = emul(ex, lg, x0, y0), bd = emul(ex, lg, x1, y1);
+      dst[2 * i] = ac ^ emul(ex, lg, 0x20, bd);
+      dst[2 * i + 1] = emul(ex, lg, x0 ^ x1, y0 ^ y1) ^ ac;
+    } else {
+      auto m16 = [&](uint16_t x, uint16_t y) -> uint16_t {
+        const uint8_t p0 = x & 0xFF, p1 = x >> 8, q0 = y & 0xFF, q1 = y >> 8;
+        const uint8_t ac = emul(ex, lg, p0, q0), bd = emul(ex, lg, p1, q1);
+        const uint8_t lo = ac ^ emul(ex, lg, 0x20, bd);
+        const uint8_t hi = emul(ex, lg, p0 ^ p1, q0 ^ q1) ^ ac;
+        return static_cast<uint16_t>(lo | (hi << 8));
+      };
+      const uint16_t xa = a[4 * i] | (a[4 * i + 1] << 8), xb = a[4 * i + 2] | (a[4 * i + 3] << 8);
+      const uint16_t ya = b[4 * i] | (b[4 * i + 1] << 8), yb = b[4 * i + 2] | (b[4 * i + 3] << 8);
+      const uint16_t ac = m16(xa, ya), bd = m16(xb, yb);
+      const uint16_t lo = ac ^ m16(0x2000, bd);
+      const uint16_t hi = m16(xa ^ xb, ya ^ yb) ^ ac;
+      dst[4 * i] = lo & 0xFF;
+      dst[4 * i + 1] = lo >> 8;
+      dst[4 * i + 2] = hi & 0xFF;
+      dst[4 * i + 3] = hi >> 8;
+    }
+  }
+}
+
+}  // namespace
+
+int sm_count() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+cudaError_t launch_matrix(int field, int groups, bool overwrite, const MatrixLaunch& a,
+                          cudaStream_t s) {
+  const int E = field_bytes(field);
+  if (E == 1) return overwrite ? launch_e<1, true>(groups, a, s) : launch_e<1, false>(groups, a, s);
+  if (E == 2) return overwrite ? launch_e<2, true>(groups, a, s) : launch_e<2, false>(groups, a, s);
+  if (E == 4) return overwrite ? launch_e<4, true>(groups, a, s) : launch_e<4, false>(groups, a, s);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_zero_rows(uint8_t* const* rows, int n, uint64_t len, cudaStream_t s) {
+  for (int j = 0; j < n; ++j) {
+    cudaError_t e = cudaMemsetAsync(rows[j], 0, len, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_xor(uint8_t* dst, const uint8_t* src, uint64_t len, cudaStream_t s) {
+  if (!len) return cudaSuccess;
+  const uint64_t ad = reinterpret_cast<uintptr_t>(dst) & 15, as = reinterpret_cast<uintptr_t>(src) & 15;
+  uint64_t head = 0, nvec = 0;
+  if (ad == as) {
+    head = (16 - ad) & 15;
+    if (head > len) head = len;
+    nvec = (len - head) / 16;
+  } else {
+    head = len;
+  }
+  const uint64_t work = nvec + head + (len - head - 16 * nvec);
+  uint64_t want = (work + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
+  xor_kernel<<<static_cast<unsigned>(want < cap ? want : cap), 256, 0, s>>>(dst, src, len, head, nvec);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
+                               uint64_t len, cudaStream_t s) {
+  if (!len) return cudaSuccess;
+  if (!g_const_ready) {
+    uint8_t ex[2][512], lg[2][256];
+    const Gf8Log* t[2] = {&gf8b_tab(), &gf8d_tab()};
+    for (int w = 0; w < 2; ++w) {
+      for (int i = 0; i < 512; ++i) ex[w][i] = t[w]->exp[i];
+      for (int i = 0; i < 256; ++i) lg[w][i] = t[w]->log[i];
+    }
+    cudaError_t e = cudaMemcpyToSymbol(c_exp, ex, sizeof(ex));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbol(c_log, lg, sizeof(lg));
+    if (e != cudaSuccess) return e;
+    g_const_ready = true;
+  }
+  const uint64_t nelem = len / field_bytes(field);
+  uint64_t want = (nelem + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
+  const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+  switch (field) {
+    case kGf8B: elementwise_kernel<kGf8B><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
+    case kGf8D: elementwise_kernel<kGf8D><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
+    case kGf16: elementwise_kernel<kGf16><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
+    case kGf32: elementwise_kernel<kGf32><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace fgfc

@@ -1,0 +1,201 @@
+/*
+ * fgf_cuda.h -- C ABI of libfgfcuda.so, the sm_100a implementation of the
+ * packed-vector `ops` AXPY family of the fgf crate (nanithefkuc/fgf 0.4.0).
+ *
+ * Every entry point here mirrors one public function of `fgf::ops`
+ * (src/ops.rs) with the same name, argument order and argument meaning, but
+ * over DEVICE buffers and stream-ordered: the call validates on the host
+ * exactly what the reference validates, then enqueues the kernels on
+ * `stream` and returns. Buffers are packed little-endian elements, as in the
+ * reference (src/ops.rs:1-39). Rust slices become (pointer, byte length)
+ * pairs; `&[(&[F::Elem], &[u8])]` terms become `fgfc_term` arrays; field
+ * elements travel as uint32_t values (the low 8/16/32 bits are used).
+ *
+ * Errors: the reference panics with an operation-named message
+ * (src/ops.rs:300-316 and each op's asserts). Here the same condition returns
+ * a nonzero `fgfc_status` and `fgfc_last_error()` returns the reference's
+ * message text for this thread. Nothing unwinds across the ABI.
+ *
+ * Aliasing: as in the reference (src/ops.rs:37-39) destinations must not
+ * alias sources; the scattered op checks its rows for overlap on the host
+ * (src/ops.rs:909-921).
+ *
+ * Allocation: entry points allocate no device memory per call. Plans own the
+ * device copy of their coefficients and prepared tables (allocated once in
+ * fgfc_plan_create); raw-coefficient calls carry their coefficients in the
+ * kernel launch parameters.
+ */
+#ifndef FGF_CUDA_H
+#define FGF_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque CUDA stream handle (a cudaStream_t); NULL is the legacy default stream. */
+typedef struct CUstream_st *fgfc_stream;
+
+/* The fields of the hot path: src/field/gf8b.rs:57, src/field/gf8d.rs:40,
+ * src/field/gf16.rs:54-60, src/field/gf32.rs:36-42. */
+typedef enum fgfc_field {
+  FGFC_GF8B = 0, /* GF(2^8) mod 0x11B, 1 byte */
+  FGFC_GF8D = 1, /* GF(2^8) mod 0x11D, 1 byte */
+  FGFC_GF16 = 2, /* (GF(2^8)/0x11B)[u]/(u^2+u+0x20), 2 bytes LE */
+  FGFC_GF32 = 3  /* GF(2^16)[v]/(v^2+v+0x2000), 4 bytes LE */
+} fgfc_field;
+
+typedef enum fgfc_status {
+  FGFC_OK = 0,
+  FGFC_ERR_WIDTH = 1,       /* "not a whole number of <F> elements"      ops.rs:301-307 */
+  FGFC_ERR_LENGTH = 2,      /* paired buffers differ in length            ops.rs:310-316 */
+  FGFC_ERR_ROWS = 3,        /* "rows is N bytes but ... need M"           ops.rs:472-477 */
+  FGFC_ERR_COEFFS = 4,      /* coefficient count does not match           ops.rs:535-541,690-696 */
+  FGFC_ERR_SOURCE = 5,      /* a source has the wrong length              ops.rs:542-550 */
+  FGFC_ERR_PLAN_DIMS = 6,   /* "plan dimensions do not match"             ops.rs:736-740 */
+  FGFC_ERR_OVERLAP = 7,     /* scattered rows overlap                     ops.rs:913-921 */
+  FGFC_ERR_BOUNDS = 8,      /* scattered row past the end of dst          ops.rs:898-902 */
+  FGFC_ERR_ALIGN = 9,       /* scattered row offset not element-aligned   ops.rs:903-907 */
+  FGFC_ERR_OVERFLOW = 10,   /* geometry overflows                         ops.rs:468-471 */
+  FGFC_ERR_ARG = 11,        /* NULL pointer / unknown field / bad handle */
+  FGFC_ERR_LIMIT = 12,      /* beyond a device limit (see fgfc_limits) */
+  FGFC_ERR_CUDA = 13,       /* a CUDA runtime call failed */
+  FGFC_ERR_NOMEM = 14       /* plan allocation failed */
+} fgfc_status;
+
+/* One `(coeffs, src)` term of the many-to-many ops (ops.rs:675-680). */
+typedef struct fgfc_term {
+  const uint32_t *coeffs; /* host array of `ncoeffs` field elements */
+  size_t ncoeffs;
+  const uint8_t *src;     /* device pointer */
+  size_t src_len;         /* bytes */
+} fgfc_term;
+
+/* A device source slice `&[u8]` for the `_with` forms. */
+typedef struct fgfc_slice {
+  const uint8_t *ptr; /* device pointer */
+  size_t len;         /* bytes */
+} fgfc_slice;
+
+/* A prepared coefficient vector or row-major matrix: `ops::Plan<F>`
+ * (ops.rs:158-276). `ops::Coeff<F>` (ops.rs:44-73) is a 1x1 plan. */
+typedef struct fgfc_plan fgfc_plan;
+
+/* Thread-local text of the last error, formatted like the reference's panic
+ * message (e.g. "mul_add: dst is 8 bytes but src is 4 bytes"). */
+const char *fgfc_last_error(void);
+const char *fgfc_version(void);
+
+/* Device limits of this build: maximum sources and rows per call. */
+void fgfc_limits(size_t *max_sources, size_t *max_rows);
+
+/* Element width in bytes (F::BYTES), or 0 for an unknown field. */
+size_t fgfc_field_bytes(fgfc_field field);
+
+/* ---------------------------------------------------------------- plans */
+
+/* Plan::matrix(rows, cols, coeffs) (ops.rs:198-212); Plan::new(coeffs) is
+ * rows = 1 (ops.rs:176-190). Coefficients are copied and prepared (device
+ * tables built and uploaded) once, here. */
+fgfc_status fgfc_plan_create(fgfc_field field, size_t rows, size_t cols, const uint32_t *coeffs,
+                             fgfc_plan **out);
+/* Coeff::new(coeff) (ops.rs:61-65): a 1x1 plan. */
+fgfc_status fgfc_coeff_create(fgfc_field field, uint32_t coeff, fgfc_plan **out);
+void fgfc_plan_destroy(fgfc_plan *plan);
+/* Plan::dimensions (ops.rs:231-233), Plan::len (ops.rs:217-219). */
+fgfc_status fgfc_plan_dimensions(const fgfc_plan *plan, size_t *rows, size_t *cols);
+size_t fgfc_plan_len(const fgfc_plan *plan);
+fgfc_field fgfc_plan_field(const fgfc_plan *plan);
+/* Plan::values (ops.rs:273-275): copies plan_len values into `out`. */
+fgfc_status fgfc_plan_values(const fgfc_plan *plan, uint32_t *out);
+/* Plan::get_at(row, col).value() (ops.rs:247-251); ERR_ARG when out of bounds. */
+fgfc_status fgfc_plan_get_at(const fgfc_plan *plan, size_t row, size_t col, uint32_t *out);
+
+/* ---------------------------------------------------------------- single row */
+
+/* add_assign / sub_assign: dst ^= src (ops.rs:323-335). */
+fgfc_status fgfc_add_assign(fgfc_field field, uint8_t *dst, size_t dst_len, const uint8_t *src,
+                            size_t src_len, fgfc_stream stream);
+/* mul_add: dst ^= coeff * src (ops.rs:342-352). */
+fgfc_status fgfc_mul_add(fgfc_field field, uint8_t *dst, size_t dst_len, uint32_t coeff,
+                         const uint8_t *src, size_t src_len, fgfc_stream stream);
+/* mul_add_with (ops.rs:359-374); `coeff` is a Coeff or any 1-entry plan. */
+fgfc_status fgfc_mul_add_with(uint8_t *dst, size_t dst_len, const fgfc_plan *coeff,
+                              const uint8_t *src, size_t src_len, fgfc_stream stream);
+/* mul_into: dst = coeff * src (ops.rs:381-392) and its prepared form (ops.rs:399-415). */
+fgfc_status fgfc_mul_into(fgfc_field field, uint8_t *dst, size_t dst_len, uint32_t coeff,
+                          const uint8_t *src, size_t src_len, fgfc_stream stream);
+fgfc_status fgfc_mul_into_with(uint8_t *dst, size_t dst_len, const fgfc_plan *coeff,
+                               const uint8_t *src, size_t src_len, fgfc_stream stream);
+/* mul_assign: dst *= coeff (ops.rs:422-432) and its prepared form (ops.rs:439-450). */
+fgfc_status fgfc_mul_assign(fgfc_field field, uint8_t *dst, size_t dst_len, uint32_t coeff,
+                            fgfc_stream stream);
+fgfc_status fgfc_mul_assign_with(uint8_t *dst, size_t dst_len, const fgfc_plan *coeff,
+                                 fgfc_stream stream);
+/* mul_elementwise: dst[i] = a[i] * b[i] (ops.rs:953-957). */
+fgfc_status fgfc_mul_elementwise(fgfc_field field, uint8_t *dst, size_t dst_len, const uint8_t *a,
+                                 size_t a_len, const uint8_t *b, size_t b_len, fgfc_stream stream);
+
+/* ---------------------------------------------------------------- one-to-many / many-to-one */
+
+/* mul_add_scatter: rows[j] ^= coeffs[j] * src (ops.rs:461-482). */
+fgfc_status fgfc_mul_add_scatter(fgfc_field field, uint8_t *rows, size_t rows_len, size_t row_len,
+                                 const uint32_t *coeffs, size_t ncoeffs, const uint8_t *src,
+                                 size_t src_len, fgfc_stream stream);
+/* mul_add_scatter_with (ops.rs:493-520). */
+fgfc_status fgfc_mul_add_scatter_with(uint8_t *rows, size_t rows_len, size_t row_len,
+                                      const fgfc_plan *plan, const uint8_t *src, size_t src_len,
+                                      fgfc_stream stream);
+/* mul_add_gather: dst ^= sum coeffs[i] * srcs[i] (ops.rs:533-555). */
+fgfc_status fgfc_mul_add_gather(fgfc_field field, uint8_t *dst, size_t dst_len,
+                                const uint32_t *coeffs, size_t ncoeffs, const fgfc_slice *srcs,
+                                size_t nsrcs, fgfc_stream stream);
+/* mul_add_gather_with (ops.rs:563-585). */
+fgfc_status fgfc_mul_add_gather_with(uint8_t *dst, size_t dst_len, const fgfc_plan *plan,
+                                     const fgfc_slice *srcs, size_t nsrcs, fgfc_stream stream);
+/* dot_product: dst = sum coeffs[i] * srcs[i] (ops.rs:597-624). */
+fgfc_status fgfc_dot_product(fgfc_field field, uint8_t *dst, size_t dst_len,
+                             const uint32_t *coeffs, size_t ncoeffs, const fgfc_slice *srcs,
+                             size_t nsrcs, fgfc_stream stream);
+/* dot_product_with (ops.rs:632-660). */
+fgfc_status fgfc_dot_product_with(uint8_t *dst, size_t dst_len, const fgfc_plan *plan,
+                                  const fgfc_slice *srcs, size_t nsrcs, fgfc_stream stream);
+
+/* ---------------------------------------------------------------- many-to-many */
+
+/* mul_add_matrix: rows[j] ^= sum_t terms[t].coeffs[j] * terms[t].src (ops.rs:675-708). */
+fgfc_status fgfc_mul_add_matrix(fgfc_field field, uint8_t *rows, size_t rows_len, size_t row_len,
+                                size_t nrows, const fgfc_term *terms, size_t nterms,
+                                fgfc_stream stream);
+/* mul_add_matrix_with: plan dimensions (nsrcs, nrows) (ops.rs:720-760). */
+fgfc_status fgfc_mul_add_matrix_with(uint8_t *rows, size_t rows_len, size_t row_len, size_t nrows,
+                                     const fgfc_plan *plan, const fgfc_slice *srcs, size_t nsrcs,
+                                     fgfc_stream stream);
+/* dot_product_matrix: overwrite form (ops.rs:773-810). */
+fgfc_status fgfc_dot_product_matrix(fgfc_field field, uint8_t *rows, size_t rows_len,
+                                    size_t row_len, size_t nrows, const fgfc_term *terms,
+                                    size_t nterms, fgfc_stream stream);
+/* dot_product_matrix_with (ops.rs:823-867): the RS encode entry point. */
+fgfc_status fgfc_dot_product_matrix_with(uint8_t *rows, size_t rows_len, size_t row_len,
+                                         size_t nrows, const fgfc_plan *plan,
+                                         const fgfc_slice *srcs, size_t nsrcs,
+                                         fgfc_stream stream);
+/* mul_add_matrix_scattered: row j at dst + row_starts[j] (ops.rs:887-941). */
+fgfc_status fgfc_mul_add_matrix_scattered(fgfc_field field, uint8_t *dst, size_t dst_len,
+                                          size_t row_len, const size_t *row_starts,
+                                          size_t nrows, const fgfc_term *terms, size_t nterms,
+                                          fgfc_stream stream);
+/* Extension with no reference counterpart (the reference has no prepared
+ * form of the scattered op, README.md:113): the same op driven by a plan of
+ * dimensions (nsrcs, nrows), as the reconstruct path uses a cached decode plan. */
+fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t *dst, size_t dst_len, size_t row_len,
+                                               const size_t *row_starts, size_t nrows,
+                                               const fgfc_plan *plan, const fgfc_slice *srcs,
+                                               size_t nsrcs, fgfc_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FGF_CUDA_H */
