@@ -1,0 +1,173 @@
+// fast_core.cuh -- device building blocks shared by the single-call kernels
+// (kernels.cu) and the persistent batch kernels (batch.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "internal.hpp"
+
+namespace fgfc {
+
+extern __shared__ __align__(16) uint8_t g_smem[];
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
+  return __byte_perm(a, b, s);
+}
+
+__device__ __forceinline__ uint32_t lds_at(uint32_t off) {
+  return *reinterpret_cast<const uint32_t*>(g_smem + off);
+}
+
+// Source loads: read-only path without L1 allocation (sources are read once).
+__device__ __forceinline__ uint4 ldg16(const uint8_t* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+
+// ---------------------------------------------------------------- byte-table layout
+//
+// Gf8 fields with at most 4 rows (one table group) and a compile-time number
+// of sources K. Sources t < kByteSrc get a full 256-entry product table (one
+// lookup per source byte, 32 KiB with the 32 lane copies; two tables share
+// each 64 KiB page, at byte offsets 0 and 128 of every 256-byte row), the
+// rest keep split-nibble tables in 4 KiB slots after the three byte-table
+// pages. With K fixed every table address is a PRMT of the data byte plus an
+// immediate.
+constexpr int kByteSrc = 6;
+constexpr int kFastMaxK = 14;
+constexpr int kFastThreads = 1024;
+constexpr uint32_t kNibbleBase = 3u * 65536u;
+
+template <int K>
+struct FastLayout {
+  static constexpr int NB = K < kByteSrc ? K : kByteSrc;  // byte-table sources
+  static constexpr int NN = K - NB;                       // nibble-table sources
+  static constexpr uint32_t tables = NN ? kNibbleBase + NN * kSlotBytes : ((NB + 1) / 2) * 65536u;
+  static constexpr uint32_t smem = tables + K * kCompactWords * 4u;  // + compact staging
+};
+
+// Expand the compact tables of K sources (plan layout: source t at
+// ((t * gstride + g0) * 32)) into the byte-table layout. `tables` is a device
+// pointer, or null to read `inl` (launch parameters). The compact words are
+// staged in shared memory first (one independent load per thread) and every
+// entry's 32 lane copies are written as 8 identical 16-byte stores.
+template <int K>
+__device__ __forceinline__ void fill_fast(const uint32_t* tables, const uint32_t* inl, uint32_t gstride,
+                                          uint32_t g0) {
+  using L = FastLayout<K>;
+  uint32_t* stage = reinterpret_cast<uint32_t*>(g_smem) + L::tables / 4;
+  for (uint32_t i = threadIdx.x; i < K * kCompactWords; i += blockDim.x) {
+    const uint32_t src = ((i >> 5) * gstride + g0) * kCompactWords + (i & 31u);
+    stage[i] = tables ? __ldg(tables + src) : inl[src];
+  }
+  __syncthreads();
+  // byte tables: word index = page * 16384 + x * 64 + half * 32 + lane
+  uint4* st4 = reinterpret_cast<uint4*>(g_smem);
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < L::NB * 2048u; i += blockDim.x) {
+    const uint32_t t = i >> 11, x = (i >> 3) & 255u, q = i & 7u;
+    const uint32_t v = stage[t * kCompactWords + (x & 15u)] ^ stage[t * kCompactWords + 16u + (x >> 4)];
+    st4[(t >> 1) * 4096u + x * 16u + (t & 1u) * 8u + q] = make_uint4(v, v, v, v);
+  }
+  if constexpr (L::NN > 0) {
+#pragma unroll 4
+    for (uint32_t i = threadIdx.x; i < L::NN * 256u; i += blockDim.x) {
+      const uint32_t v =
+          stage[(L::NB + (i >> 8)) * kCompactWords + ((i >> 3) & 1u) * 16u + ((i >> 4) & 15u)];
+      st4[kNibbleBase / 16 + i] = make_uint4(v, v, v, v);
+    }
+  }
+  __syncthreads();
+}
+
+// Lane / page registers of the byte-table layout.
+struct FastRegs {
+  uint32_t lrp[3];  // byte-table pages 0..2
+  uint32_t lrn;     // nibble slots (page 3)
+  __device__ __forceinline__ FastRegs() {
+    const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) lrp[p] = lane4 | (static_cast<uint32_t>(p) << 16);
+    lrn = lane4 | (3u << 16);
+  }
+};
+
+// Fold NW words (4 bytes each, byte b of word q is element 4q + b) of each
+// of the K sources into acc (acc[e] = products for rows 0..3 of element e).
+template <int K, int NW>
+__device__ __forceinline__ void fast_fold(const uint32_t (&w)[K][NW], uint32_t (&acc)[4 * NW],
+                                          const FastRegs& r) {
+  using L = FastLayout<K>;
+#pragma unroll
+  for (int t = 0; t < L::NB; t += 2) {
+    const uint32_t lr = r.lrp[t >> 1];
+    if (t + 1 < L::NB) {
+#pragma unroll
+      for (int q = 0; q < NW; ++q)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+          acc[4 * q + b] ^= lds_at(prmt(w[t][q], lr, sel)) ^ lds_at(prmt(w[t + 1][q], lr, sel) + 128u);
+        }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NW; ++q)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+          acc[4 * q + b] ^= lds_at(prmt(w[t][q], lr, sel));
+        }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < L::NN; ++i) {
+    const uint32_t pat = ((static_cast<uint32_t>(48 + i) & 15u) << 4) * 0x01010101u;
+#pragma unroll
+    for (int q = 0; q < NW; ++q) {
+      const uint32_t xl = (w[L::NB + i][q] & 0x0F0F0F0Fu) | pat;
+      const uint32_t xh = ((w[L::NB + i][q] >> 4) & 0x0F0F0F0Fu) | pat;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+        acc[4 * q + b] ^= lds_at(prmt(xl, r.lrn, sel)) ^ lds_at(prmt(xh, r.lrn, sel) + 128u);
+      }
+    }
+  }
+}
+
+// Row rr (0..3) of one output word from 4 element accumulators (4x4 byte
+// transpose: acc[e] holds rows 0..3 of element e).
+__device__ __forceinline__ uint32_t row_word4(const uint32_t* acc, int rr) {
+  const uint32_t s01 = prmt(acc[0], acc[1], rr < 2 ? 0x5140u : 0x7362u);
+  const uint32_t s23 = prmt(acc[2], acc[3], rr < 2 ? 0x5140u : 0x7362u);
+  return prmt(s01, s23, (rr & 1) ? 0x7632u : 0x5410u);
+}
+
+// Store one 16-byte column of up to 4 rows; accumulate unless overwriting.
+__device__ __forceinline__ void store_col4(const uint32_t (&acc)[16], uint8_t* const* dst, uint32_t nrows,
+                                           uint64_t off, bool ovr) {
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr) {
+    if (rr >= static_cast<int>(nrows)) break;
+    uint4 o;
+    o.x = row_word4(&acc[0], rr);
+    o.y = row_word4(&acc[4], rr);
+    o.z = row_word4(&acc[8], rr);
+    o.w = row_word4(&acc[12], rr);
+    uint4* dp = reinterpret_cast<uint4*>(dst[rr] + off);
+    if (!ovr) {
+      const uint4 dv = *dp;
+      o.x ^= dv.x;
+      o.y ^= dv.y;
+      o.z ^= dv.z;
+      o.w ^= dv.w;
+    }
+    *dp = o;
+  }
+}
+
+}  // namespace fgfc

@@ -20,7 +20,7 @@ constexpr int kMaxRows = 64;
 // of the lo-nibble word (bytes 0..127) and of the hi-nibble word (128..255),
 // so a warp's 32 lookups hit 32 distinct banks.
 constexpr int kSlotBytes = 4096;
-constexpr int kMaxSlots = 56;            // 224 KiB of tables per CTA
+constexpr int kMaxSlots = 54;            // 216 KiB of tables (+ 6.75 KiB staging) per CTA
 constexpr int kInlineSlots = 48;         // tables carried in launch parameters
 constexpr int kCompactWords = 32;        // 16 lo + 16 hi words per slot
 

@@ -21,40 +21,33 @@
 
 #include <cstdint>
 
+#include "fast_core.cuh"
 #include "internal.hpp"
 
 namespace fgfc {
 
-extern __shared__ __align__(16) uint8_t g_smem[];
-
 namespace {
-
-__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
-  return __byte_perm(a, b, s);
-}
-
-__device__ __forceinline__ uint32_t lds_at(uint32_t off) {
-  return *reinterpret_cast<const uint32_t*>(g_smem + off);
-}
-
-__device__ __forceinline__ uint4 ldg16(const uint8_t* p) {
-  return __ldg(reinterpret_cast<const uint4*>(p));
-}
 
 // Copy compact tables for this launch into the replicated shared layout:
 // word index i of the shared area is slot (i >> 10), nibble row
-// ((i >> 6) & 15), half ((i >> 5) & 1), lane (i & 31).
+// ((i >> 6) & 15), half ((i >> 5) & 1), lane (i & 31). The compact words are
+// staged in shared memory first (one independent load per thread) and each
+// entry's 32 lane copies are written as 8 identical 16-byte stores.
 template <int E, int G>
 __device__ __forceinline__ void fill_tables(const MatrixLaunch& a) {
-  const uint32_t nwords = a.k * E * G * 1024u;
-  uint32_t* st = reinterpret_cast<uint32_t*>(g_smem);
-  for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) {
-    const uint32_t slot = i >> 10;                 // (t * E + p) * G + g
-    const uint32_t g = slot % G;
-    const uint32_t tp = slot / G;
-    const uint32_t word = ((i >> 5) & 1u) * 16u + ((i >> 6) & 15u);
-    const uint32_t src = (tp * a.gstride + a.g0 + g) * kCompactWords + word;
-    st[i] = a.tables ? __ldg(a.tables + src) : a.inline_tab[src];
+  const uint32_t nslots = a.k * E * G;
+  uint32_t* stage = reinterpret_cast<uint32_t*>(g_smem) + nslots * 1024u;
+  for (uint32_t i = threadIdx.x; i < nslots * kCompactWords; i += blockDim.x) {
+    const uint32_t slot = i >> 5;  // (t * E + p) * G + g
+    const uint32_t src = ((slot / G) * a.gstride + a.g0 + slot % G) * kCompactWords + (i & 31u);
+    stage[i] = a.tables ? __ldg(a.tables + src) : a.inline_tab[src];
+  }
+  __syncthreads();
+  uint4* st4 = reinterpret_cast<uint4*>(g_smem);
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < nslots * 256u; i += blockDim.x) {
+    const uint32_t v = stage[(i >> 8) * kCompactWords + ((i >> 3) & 1u) * 16u + ((i >> 4) & 15u)];
+    st4[i] = make_uint4(v, v, v, v);
   }
 }
 
@@ -228,140 +221,32 @@ __global__ void __launch_bounds__(256) matrix_scalar_kernel(const __grid_constan
 
 // ---------------------------------------------------------------- byte-table kernel
 //
-// Gf8 fields with at most 4 rows (one table group) and a compile-time number
-// of sources K: the RS(10,4) encode / reconstruct shape and the single-row
-// ops. Sources t < kByteSrc get a full 256-entry product table (one lookup
-// per source byte, 32 KiB with the 32 lane copies; two tables share each
-// 64 KiB page, at byte offsets 0 and 128 of every 256-byte row), the rest
-// keep split-nibble tables in 4 KiB slots after the three byte-table pages.
-// With K fixed every table address is a PRMT of the data byte plus an
-// immediate, and the next column's sources are prefetched into registers
-// while the current one is folded.
-constexpr int kByteSrc = 6;
-constexpr uint32_t kNibbleBase = 3u * 65536u;
-// Rows shorter than this (in 16-byte vectors) use the nibble kernel: the
-// byte tables cost about a microsecond per CTA to fill.
+// Gf8, at most 4 rows, K <= 14 sources: the RS(10,4) encode / reconstruct
+// shape and the single-row ops (fast_core.cuh). Rows shorter than
+// kFastMinVec vectors use the nibble kernel, whose tables fill faster.
 constexpr uint64_t kFastMinVec = 1u << 18;  // 4 MiB
 
-template <int K>
-struct FastLayout {
-  static constexpr int NB = K < kByteSrc ? K : kByteSrc;  // byte-table sources
-  static constexpr int NN = K - NB;                       // nibble-table sources
-  static constexpr uint32_t smem = NN ? kNibbleBase + NN * kSlotBytes : ((NB + 1) / 2) * 65536u;
-};
-
-template <int K>
-__device__ __forceinline__ void fill_fast_tables(const MatrixLaunch& a) {
-  using L = FastLayout<K>;
-  uint32_t* st = reinterpret_cast<uint32_t*>(g_smem);
-  auto compact = [&](uint32_t t, uint32_t w) -> uint32_t {
-    const uint32_t i = t * a.gstride * kCompactWords + a.g0 * kCompactWords + w;
-    return a.tables ? __ldg(a.tables + i) : a.inline_tab[i];
-  };
-  // byte tables: word index = page * 16384 + x * 64 + half * 32 + lane
-  for (uint32_t i = threadIdx.x; i < L::NB * 8192u; i += blockDim.x) {
-    const uint32_t t = i >> 13, x = (i >> 5) & 255u, lane = i & 31u;
-    st[(t >> 1) * 16384u + x * 64u + (t & 1u) * 32u + lane] =
-        compact(t, x & 15u) ^ compact(t, 16u + (x >> 4));
-  }
-  // nibble slots for sources NB..K-1
-  for (uint32_t i = threadIdx.x; i < L::NN * 1024u; i += blockDim.x) {
-    const uint32_t s = i >> 10;
-    st[kNibbleBase / 4 + i] = compact(L::NB + s, ((i >> 5) & 1u) * 16u + ((i >> 6) & 15u));
-  }
-}
-
-template <int K, bool OVR, bool PREFETCH>
-__global__ void __launch_bounds__(512, 1) matrix_fast_kernel(const __grid_constant__ MatrixLaunch a) {
-  using L = FastLayout<K>;
-  fill_fast_tables<K>(a);
-  __syncthreads();
-  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
-  uint32_t lrp[3];
-#pragma unroll
-  for (int p = 0; p < 3; ++p) lrp[p] = lane4 | (static_cast<uint32_t>(p) << 16);
-  const uint32_t lrn = lane4 | (3u << 16);  // nibble slots live in page 3
+template <int K, bool OVR>
+__global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __grid_constant__ MatrixLaunch a) {
+  fill_fast<K>(a.tables, a.inline_tab, a.gstride, a.g0);
+  const FastRegs r;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  uint4 nxt[K];
-  if (PREFETCH && v < a.nvec) {
-#pragma unroll
-    for (int t = 0; t < K; ++t) nxt[t] = ldg16(a.src[t] + a.head + v * 16u);
-  }
-  for (; v < a.nvec; v += stride) {
+  for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < a.nvec; v += stride) {
     const uint64_t off = a.head + v * 16u;
-    uint4 cur[K];
+    uint32_t w[K][4];
 #pragma unroll
-    for (int t = 0; t < K; ++t) cur[t] = PREFETCH ? nxt[t] : ldg16(a.src[t] + off);
-    if (PREFETCH && v + stride < a.nvec) {
-#pragma unroll
-      for (int t = 0; t < K; ++t) nxt[t] = ldg16(a.src[t] + off + stride * 16u);
+    for (int t = 0; t < K; ++t) {
+      const uint4 x = ldg16(a.src[t] + off);
+      w[t][0] = x.x;
+      w[t][1] = x.y;
+      w[t][2] = x.z;
+      w[t][3] = x.w;
     }
     uint32_t acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0;
-    // byte-table sources, in pairs sharing one page
-#pragma unroll
-    for (int t = 0; t < L::NB; t += 2) {
-      const uint32_t lr = lrp[t >> 1];
-      const uint32_t wa[4] = {cur[t].x, cur[t].y, cur[t].z, cur[t].w};
-      if (t + 1 < L::NB) {
-        const uint32_t wb[4] = {cur[t + 1].x, cur[t + 1].y, cur[t + 1].z, cur[t + 1].w};
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
-            acc[4 * q + b] ^= lds_at(prmt(wa[q], lr, sel)) ^ lds_at(prmt(wb[q], lr, sel) + 128u);
-          }
-      } else {
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
-            acc[4 * q + b] ^= lds_at(prmt(wa[q], lr, sel));
-          }
-      }
-    }
-    // nibble-table sources
-#pragma unroll
-    for (int i = 0; i < L::NN; ++i) {
-      const uint32_t pat = ((static_cast<uint32_t>(48 + i) & 15u) << 4) * 0x01010101u;
-      const uint32_t w4[4] = {cur[L::NB + i].x, cur[L::NB + i].y, cur[L::NB + i].z, cur[L::NB + i].w};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t xl = (w4[q] & 0x0F0F0F0Fu) | pat;
-        const uint32_t xh = ((w4[q] >> 4) & 0x0F0F0F0Fu) | pat;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
-          acc[4 * q + b] ^= lds_at(prmt(xl, lrn, sel)) ^ lds_at(prmt(xh, lrn, sel) + 128u);
-        }
-      }
-    }
-    // 4x4 byte transposes: acc[e] holds rows 0..3 of element e
-#pragma unroll
-    for (int rr = 0; rr < 4; ++rr) {
-      if (rr >= static_cast<int>(a.nrows)) break;
-      uint4 o;
-      uint32_t* ow = &o.x;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t s01 = prmt(acc[4 * q], acc[4 * q + 1], rr < 2 ? 0x5140u : 0x7362u);
-        const uint32_t s23 = prmt(acc[4 * q + 2], acc[4 * q + 3], rr < 2 ? 0x5140u : 0x7362u);
-        ow[q] = prmt(s01, s23, (rr & 1) ? 0x7632u : 0x5410u);
-      }
-      uint4* dp = reinterpret_cast<uint4*>(a.dst[rr] + off);
-      if (!OVR) {
-        const uint4 dv = *dp;
-        o.x ^= dv.x;
-        o.y ^= dv.y;
-        o.z ^= dv.z;
-        o.w ^= dv.w;
-      }
-      *dp = o;
-    }
+    fast_fold<K, 4>(w, acc, r);
+    store_col4(acc, a.dst, a.nrows, off, OVR);
   }
 }
 
@@ -369,19 +254,18 @@ int g_sms = 0;
 
 template <int K, bool OVR>
 cudaError_t launch_fast_k(const MatrixLaunch& a, cudaStream_t s) {
-  constexpr bool PF = K <= 10;
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR, PF>,
+    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          FastLayout<K>::smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const uint64_t want = (a.nvec + 511) / 512;
+  const uint64_t want = (a.nvec + kFastThreads - 1) / kFastThreads;
   const uint64_t cap = static_cast<uint64_t>(sm_count());
   const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
-  matrix_fast_kernel<K, OVR, PF><<<blocks, 512, FastLayout<K>::smem, s>>>(a);
+  matrix_fast_kernel<K, OVR><<<blocks, kFastThreads, FastLayout<K>::smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -413,14 +297,15 @@ cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kMaxSlots * kSlotBytes);
+                                         kMaxSlots * (kSlotBytes + kCompactWords * 4));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(matrix_scalar_kernel<E, G, OVR>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSlots * kSlotBytes);
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kMaxSlots * (kSlotBytes + kCompactWords * 4));
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const size_t smem = static_cast<size_t>(a.k) * E * G * kSlotBytes;
+  const size_t smem = static_cast<size_t>(a.k) * E * G * (kSlotBytes + kCompactWords * 4);
   const int sms = sm_count();
   if (E == 1 && G == 1 && a.k <= 14 && a.nvec >= kFastMinVec) {
     cudaError_t e = launch_fast<OVR>(a, s);
