@@ -1,0 +1,427 @@
+"""Benchmark: RS(10,4) Gf8D encode + reconstruct of a batch of device-resident
+stripes (256 stripes x 1 MiB shards), through the batched C-ABI path.
+
+One step = one batched `dot_product_matrix_with` submission that encodes every
+stripe (10 data shards -> 4 parity shards, Cauchy matrix c[i][j] =
+inv(x_i + y_j), x_i = 10 + i, y_j = j) followed by one batched
+`mul_add_matrix_scattered` submission that rebuilds 4 seeded-random erased
+shards of every stripe in place from 10 survivors (decode plans from host
+Gauss-Jordan inversion, cached per erasure pattern). The metric is source
+GB/s: the source bytes both operations read (10 shards each, per stripe) per
+second, whole job.
+
+python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Under torchrun each rank runs its own batch (weak scaling, no collective on
+the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "RS(10,4) Gf8D encode+reconstruct source GB/s (batched, device-resident)"
+K_SRC, M_PAR, N_ALL = 10, 4, 14
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--stripes", type=int, default=256)
+    p.add_argument("--shard-mib", type=float, default=1.0)
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="bounded CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def erasure_patterns(nst: int, seed: int = 0x5EED):
+    rng = np.random.default_rng(seed)
+    return [tuple(sorted(rng.choice(N_ALL, size=M_PAR, replace=False).tolist())) for _ in range(nst)]
+
+
+def config(args, L):
+    return {
+        "workload": f"RS(10,4) Gf8D, {args.stripes} stripes x {L >> 10} KiB shards: batched encode "
+                    f"(dot_product_matrix_with) + reconstruct of 4 seeded erasures per stripe "
+                    f"(mul_add_matrix_scattered with cached decode plans)",
+        "field": "Gf8D (0x11D)", "k": K_SRC, "m": M_PAR, "stripes_per_gpu": args.stripes,
+        "shard_bytes": L, "matrix": "Cauchy inv(x_i + y_j), x_i = 10 + i, y_j = j",
+        "l2": "inputs (%.1f GiB per GPU) larger than L2 (126 MB)" % (args.stripes * N_ALL * L / 2 ** 30),
+        "parallelism": f"replicas x{args.gpus} (stripes sharded across ranks, no collective)",
+    }
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle port)
+
+class PortJob(C.Structure):
+    _fields_ = [("field", C.c_int), ("k", C.c_size_t), ("m", C.c_size_t), ("row_len", C.c_size_t),
+                ("coeffs", C.c_void_p), ("srcs", C.c_void_p), ("rows", C.c_void_p), ("overwrite", C.c_int)]
+
+
+def cpu_baseline(L: int, seconds: float, nstripes: int = 16):
+    """Times the C restatement of the reference's AVX2+GFNI blocked kernels
+    (oracle/cpu_port.c) on a bounded sample of the same workload, all host
+    threads, one stripe per job."""
+    from oracle import orc
+    from fgf_b200 import fields
+
+    lib = orc.L()
+    lib.orc_port_supported.restype = C.c_int
+    if not lib.orc_port_supported():
+        return None
+    cores = os.cpu_count() or 1
+    gf = fields.Gf8D
+    cm = fields.cauchy(gf, M_PAR, K_SRC)
+    enc = np.array(fields.encode_plan_coeffs(cm)[2], dtype=np.uint32)
+    pats = erasure_patterns(nstripes, seed=0xC0DE)
+    keep, jobs = [enc], []
+    for s in range(nstripes):
+        code = [orc.noise(L, 1000 * s + r) for r in range(N_ALL)]
+        keep.append(code)
+        sp = (C.c_void_p * K_SRC)(*[code[t].ctypes.data for t in range(K_SRC)])
+        rp = (C.c_void_p * M_PAR)(*[code[K_SRC + j].ctypes.data for j in range(M_PAR)])
+        keep += [sp, rp]
+        jobs.append(PortJob(1, K_SRC, M_PAR, L, enc.ctypes.data, C.cast(sp, C.c_void_p),
+                            C.cast(rp, C.c_void_p), 1))
+        er = list(pats[s])
+        sv = [i for i in range(N_ALL) if i not in er][:K_SRC]
+        dm = fields.decode_rows(gf, cm, sv, er)
+        dco = np.array([dm[j][t] for t in range(K_SRC) for j in range(M_PAR)], dtype=np.uint32)
+        sp2 = (C.c_void_p * K_SRC)(*[code[i].ctypes.data for i in sv])
+        rp2 = (C.c_void_p * M_PAR)(*[code[e].ctypes.data for e in er])
+        keep += [dco, sp2, rp2]
+        jobs.append(PortJob(1, K_SRC, M_PAR, L, dco.ctypes.data, C.cast(sp2, C.c_void_p),
+                            C.cast(rp2, C.c_void_p), 0))
+    arr = (PortJob * len(jobs))(*jobs)
+    lib.orc_port_run_jobs(arr, C.c_size_t(len(jobs)), cores)  # warm-up (page faults)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        lib.orc_port_run_jobs(arr, C.c_size_t(len(jobs)), cores)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    src_bytes = reps * nstripes * 2 * K_SRC * L
+    return {"value": round(src_bytes / el / 1e9, 2), "unit": "GB/s", "cores": cores, "kind": "port",
+            "sample": f"{nstripes} stripes x RS(10,4) x {L >> 10} KiB encode+reconstruct, repeated {reps}x "
+                      f"for {el:.1f} s on {cores} threads (oracle/cpu_port.c: AVX2+GFNI restatement of "
+                      f"the reference's blocked kernels; the reference is Rust and not buildable here)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    L = int(args.shard_mib * 2 ** 20)
+    per = max(1.0, args.cpu_seconds / max(1, args.steps))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(L, per if i >= args.warmup else 0.5)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "host CPU lacks AVX2+GFNI"}))
+            return 0
+        if i >= args.warmup:
+            vals.append(r)
+    v = float(np.median([x["value"] for x in vals]))
+    base = dict(vals[-1])
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded LCG bytes)",
+            "config": config(args, L), "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [[x.strip() for x in r.split(",")] for r in out.strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per step of the dominant kernels from the committed ncu
+    summary (profiles/traffic.txt, `key: bytes` lines), or None."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("rs104_batch_bytes_per_step:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def run_ours(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from fgf_b200 import batch as fb
+    from fgf_b200 import ops
+    from fgf_b200.fields import Gf8D, cauchy, decode_rows, encode_plan_coeffs
+
+    L = int(args.shard_mib * 2 ** 20)
+    nst = args.stripes
+    stripe = N_ALL * L
+    code = torch.empty(nst * stripe, dtype=torch.uint8, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0x1234 + rank)
+    code.random_(0, 256, generator=g)
+    cm = cauchy(Gf8D, M_PAR, K_SRC)
+    enc_plan = ops.Plan.matrix(Gf8D, *encode_plan_coeffs(cm))
+    pats = erasure_patterns(nst, seed=0x5EED + rank)
+    cache = {}
+
+    def dec_plan(er):
+        if er not in cache:
+            sv = [i for i in range(N_ALL) if i not in er][:K_SRC]
+            dm = decode_rows(Gf8D, cm, sv, list(er))
+            cache[er] = (ops.Plan.matrix(Gf8D, K_SRC, M_PAR, [dm[j][t] for t in range(K_SRC)
+                                                                for j in range(M_PAR)]), sv)
+        return cache[er]
+
+    def row(s, r):
+        return code[s * stripe + r * L: s * stripe + (r + 1) * L]
+
+    enc_jobs = [fb.Job(enc_plan, [row(s, t) for t in range(K_SRC)],
+                       code[s * stripe + K_SRC * L: (s + 1) * stripe], L, M_PAR, True) for s in range(nst)]
+    rec_jobs = []
+    for s in range(nst):
+        plan, sv = dec_plan(pats[s])
+        rec_jobs.append(fb.Job(plan, [row(s, i) for i in sv], code[s * stripe:(s + 1) * stripe], L, M_PAR,
+                               False, [e * L for e in pats[s]]))
+    bt = fb.Batch(graphs=True)
+    enc_p, rec_p = bt.prepare(enc_jobs), bt.prepare(rec_jobs)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- correctness of one step (encode vs oracle on stripe 0; reconstruct
+    # restores erased shards bit-exactly on sampled stripes)
+    bt.run_prepared(enc_p, stream)
+    torch.cuda.synchronize()
+    check = list(range(0, nst, max(1, nst // 8)))
+    truth = {s: [row(s, e).cpu().numpy().copy() for e in pats[s]] for s in check}
+    for s in range(nst):
+        for e in pats[s]:
+            row(s, e).zero_()
+    bt.run_prepared(rec_p, stream)
+    torch.cuda.synchronize()
+    ok = all(np.array_equal(row(s, e).cpu().numpy(), truth[s][j]) for s in check for j, e in enumerate(pats[s]))
+    if rank == 0:
+        from oracle import orc
+
+        h0 = code[:stripe].cpu().numpy()
+        want = np.zeros(M_PAR * L, np.uint8)
+        orc.dot_product_matrix(1, want, L, M_PAR, encode_plan_coeffs(cm)[2],
+                               [h0[t * L:(t + 1) * L].copy() for t in range(K_SRC)])
+        ok = ok and np.array_equal(h0[K_SRC * L:], want)
+    if not ok:
+        print(json.dumps({"metric": METRIC, "error": "parity check failed"}))
+        return 1
+
+    # ---- timed region: W warm-up steps, K timed steps, events per submission
+    for _ in range(args.warmup):
+        bt.run_prepared(enc_p, stream)
+        bt.run_prepared(rec_p, stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    torch.cuda.synchronize()
+    start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        bt.run_prepared(enc_p, stream)
+        launches += bt.stats()["launches"]
+        ev[i][1].record(stream)
+        bt.run_prepared(rec_p, stream)
+        launches += bt.stats()["launches"]
+        ev[i][2].record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = start.elapsed_time(end)
+    enc_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
+    rec_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    src_per_step = nst * 2 * K_SRC * L * world
+    value = src_per_step / (ms_step / 1e3) / 1e9
+
+    # ---- roofline of the dominant kernels (byte-table batch kernels, K = 10)
+    peak, peak_kind = hbm_peak()
+    enc_bytes = nst * (K_SRC + M_PAR) * L            # read 10, write 4
+    rec_bytes = nst * (K_SRC + 2 * M_PAR) * L        # read 10, read+write 4
+    achieved = (enc_bytes + rec_bytes) / ((enc_ms + rec_ms) / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": profiled_traffic(), "algorithmic_bytes_per_step": enc_bytes + rec_bytes,
+            "encode": {"ms": round(enc_ms, 4), "GB/s": round(enc_bytes / enc_ms / 1e6, 1),
+                       "frac": round(enc_bytes / enc_ms / 1e6 / peak, 4),
+                       "source_GB/s": round(nst * K_SRC * L / enc_ms / 1e6, 1),
+                       "kernel": "batch_fast_uniform_kernel<10> (one plan for every stripe)"},
+            "reconstruct": {"ms": round(rec_ms, 4), "GB/s": round(rec_bytes / rec_ms / 1e6, 1),
+                            "frac": round(rec_bytes / rec_ms / 1e6 / peak, 4),
+                            "source_GB/s": round(nst * K_SRC * L / rec_ms / 1e6, 1),
+                            "kernel": "batch_fast_kernel<10> (work-list, per-stripe decode plans)"},
+            "note": "achieved = algorithmic bytes of both submissions / their CUDA-event time"}
+
+    # ---- e2e: host buffers through the public API, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        cv = code.view(nst, N_ALL * L)
+        host_in = torch.empty(nst, K_SRC * L, dtype=torch.uint8).pin_memory()
+        host_in.copy_(cv[:, :K_SRC * L].cpu())
+        host_par = torch.empty(nst, M_PAR * L, dtype=torch.uint8).pin_memory()
+        host_rec = torch.empty(nst, M_PAR, L, dtype=torch.uint8).pin_memory()
+
+        def e2e_step():
+            for s in range(nst):
+                cv[s, :K_SRC * L].copy_(host_in[s], non_blocking=True)
+            bt.run_prepared(enc_p, stream)
+            bt.run_prepared(rec_p, stream)
+            for s in range(nst):
+                host_par[s].copy_(cv[s, K_SRC * L:], non_blocking=True)
+                for j, e in enumerate(pats[s]):
+                    host_rec[s, j].copy_(row(s, e), non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        es = max(1, min(args.steps, 5))
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(es):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": round(src_per_step / (ems / es / 1e3) / 1e9, 2), "unit": "GB/s",
+               "h2d_bytes_per_step": nst * K_SRC * L * world, "d2h_bytes_per_step": 2 * nst * M_PAR * L * world,
+               "steps": es, "note": "pinned host shards in, parity and rebuilt shards out, per step"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and world == 1:
+        cpu = cpu_baseline(L, args.cpu_seconds)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded uniform random bytes; seeded erasure patterns)",
+            "config": config(args, L), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clocks, "parity_check": "passed"}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

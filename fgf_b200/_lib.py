@@ -36,9 +36,10 @@ class MatrixJob(C.Structure):
 
     _fields_ = [
         ("plan", C.c_void_p),
-        ("srcs", C.POINTER(c_u8p)),
+        ("srcs", C.POINTER(Slice)),
         ("nsrcs", c_size),
         ("dst", c_u8p),
+        ("dst_len", c_size),
         ("row_starts", C.POINTER(c_size)),
         ("nrows", c_size),
         ("row_len", c_size),
@@ -88,6 +89,11 @@ _SIGS = {
                                                  C.POINTER(Term), c_size, c_stream]),
     "fgfc_mul_add_matrix_scattered_with": (c_status, [c_u8p, c_size, c_size, C.POINTER(c_size), c_size,
                                                       C.c_void_p, C.POINTER(Slice), c_size, c_stream]),
+    "fgfc_batch_create": (c_status, [C.POINTER(C.c_void_p)]),
+    "fgfc_batch_destroy": (None, [C.c_void_p]),
+    "fgfc_batch_set_graphs": (c_status, [C.c_void_p, C.c_int]),
+    "fgfc_batch_run": (c_status, [C.c_void_p, C.POINTER(MatrixJob), c_size, c_stream]),
+    "fgfc_batch_stats": (c_status, [C.c_void_p, C.POINTER(c_size), C.POINTER(c_size), C.POINTER(C.c_int)]),
 }
 
 _lib: C.CDLL | None = None

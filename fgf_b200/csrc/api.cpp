@@ -792,3 +792,130 @@ fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t* dst, size_t dst_len, siz
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- batches
+
+struct fgfc_batch {
+  void* state;
+};
+
+extern "C" {
+
+fgfc_status fgfc_batch_create(fgfc_batch** out) {
+  if (!out) return fail(FGFC_ERR_ARG, "batch: null argument");
+  *out = new fgfc_batch{batch_state_create()};
+  return ok();
+}
+
+void fgfc_batch_destroy(fgfc_batch* batch) {
+  if (!batch) return;
+  batch_state_destroy(batch->state);
+  delete batch;
+}
+
+fgfc_status fgfc_batch_set_graphs(fgfc_batch* batch, int enable) {
+  if (!batch) return fail(FGFC_ERR_ARG, "batch: null batch");
+  batch_state_graphs(batch->state, enable != 0);
+  return ok();
+}
+
+fgfc_status fgfc_batch_stats(const fgfc_batch* batch, size_t* launches, size_t* items,
+                             int* graph_replayed) {
+  if (!batch) return fail(FGFC_ERR_ARG, "batch: null batch");
+  batch_state_stats(batch->state, launches, items, graph_replayed);
+  return ok();
+}
+
+// Every job is validated exactly as the single call it stands for
+// (src/ops.rs:720-867 contiguous, 887-941 scattered), then lowered to
+// sub-jobs of at most 4 table groups.
+fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_t njobs,
+                           fgfc_stream stream) {
+  if (!batch || (njobs && !jobs)) return fail(FGFC_ERR_ARG, "batch: null argument");
+  std::vector<LoweredJob> low;
+  low.reserve(njobs);
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_matrix_job& J = jobs[i];
+    const char* name = J.row_starts ? "mul_add_matrix_scattered_with"
+                                    : (J.overwrite ? "dot_product_matrix_with" : "mul_add_matrix_with");
+    fgfc_status st;
+    const fgfc_plan* plan = J.plan;
+    if (!plan) return fail(FGFC_ERR_ARG, "batch job %zu: %s: null plan", i, name);
+    const int field = plan->field;
+    if (J.row_starts) {
+      if (J.overwrite)
+        return fail(FGFC_ERR_ARG, "batch job %zu: scattered rows accumulate; overwrite is not defined", i);
+      if (!check_scattered_rows(field, name, J.dst_len, J.row_len, J.row_starts, J.nrows, &st)) {
+        t_err = "batch job " + std::to_string(i) + ": " + t_err;
+        return st;
+      }
+    } else {
+      if (!check_width(field, name, J.row_len, &st)) {
+        t_err = "batch job " + std::to_string(i) + ": " + t_err;
+        return st;
+      }
+      size_t used;
+      if (mul_overflows(J.nrows, J.row_len, &used))
+        return fail(FGFC_ERR_OVERFLOW, "batch job %zu: %s: row geometry overflows", i, name);
+      if (J.dst_len < used)
+        return fail(FGFC_ERR_ROWS, "batch job %zu: %s: rows is %zu bytes but %zu rows of %zu bytes need %zu",
+                    i, name, J.dst_len, J.nrows, J.row_len, used);
+    }
+    if (plan->rows != J.nsrcs || plan->cols != J.nrows)
+      return fail(FGFC_ERR_PLAN_DIMS, "batch job %zu: %s: plan dimensions do not match (sources, rows)", i,
+                  name);
+    if (J.nsrcs && !J.srcs) return fail(FGFC_ERR_ARG, "batch job %zu: %s: null sources", i, name);
+    for (size_t t = 0; t < J.nsrcs; ++t)
+      if (J.srcs[t].len != J.row_len)
+        return fail(FGFC_ERR_SOURCE, "batch job %zu: %s: source %zu is %zu bytes, expected %zu", i, name, t,
+                    J.srcs[t].len, J.row_len);
+    if (J.nrows == 0 || J.row_len == 0) continue;
+    if (J.nsrcs == 0) {
+      if (J.overwrite) {
+        cudaError_t e = cudaMemsetAsync(J.dst, 0, J.nrows * J.row_len, stream);
+        if (e != cudaSuccess) return cuda_fail(e, name);
+      }
+      continue;
+    }
+    const int E = field_bytes(field);
+    const int R = 4 / E;
+    std::vector<uint64_t> dsts(J.nrows);
+    for (size_t j = 0; j < J.nrows; ++j)
+      dsts[j] = reinterpret_cast<uint64_t>(J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len));
+    std::vector<uint64_t> srcs(J.nsrcs);
+    const uintptr_t al = reinterpret_cast<uintptr_t>(J.srcs[0].ptr) & 15;
+    bool same = (al % E) == 0;
+    for (size_t t = 0; t < J.nsrcs; ++t) {
+      srcs[t] = reinterpret_cast<uint64_t>(J.srcs[t].ptr);
+      same = same && (srcs[t] & 15) == al;
+    }
+    for (uint64_t d : dsts) same = same && (d & 15) == al;
+    uint64_t head = J.row_len, nvec = 0;
+    if (same) {
+      head = std::min<uint64_t>((16 - al) & 15, J.row_len);
+      nvec = (J.row_len - head) / 16;
+    }
+    const size_t gtot = (J.nrows + R - 1) / R;
+    for (size_t g0 = 0; g0 < gtot; g0 += 4) {
+      LoweredJob L;
+      L.field = field;
+      L.tables = plan->dev + plan->off_mat;
+      L.gstride = plan->mat_groups;
+      L.g0 = g0;
+      L.G = std::min<size_t>(4, gtot - g0);
+      L.len = J.row_len;
+      L.head = head;
+      L.nvec = nvec;
+      L.k = J.nsrcs;
+      L.nrows = std::min(J.nrows - g0 * R, L.G * R);
+      L.ovr = J.overwrite != 0;
+      L.srcs = srcs;
+      L.dsts.assign(dsts.begin() + g0 * R, dsts.begin() + g0 * R + L.nrows);
+      low.push_back(std::move(L));
+    }
+  }
+  cudaError_t e = batch_run(batch->state, low, stream);
+  return e == cudaSuccess ? ok() : cuda_fail(e, "batch");
+}
+
+}  // extern "C"

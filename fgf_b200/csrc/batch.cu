@@ -1,0 +1,834 @@
+// batch.cu -- batched submissions: many stripes of uneven field, k, m and
+// shard length in one persistent launch per class, driven by a device
+// work-list.
+//
+// A submission is lowered on the host to sub-jobs (all sources of a stripe,
+// the rows of at most 4 table groups) and grouped in classes:
+//   * Gf8 sub-jobs of at most 4 rows and K <= 14 sources use the byte-table
+//     layout (fast_core.cuh), one class per K. When every sub-job of such a
+//     class shares one plan, the CTAs load the tables once and grid-stride
+//     over the flattened columns of all stripes (the stripes travel in the
+//     launch parameters); otherwise they claim work items.
+//   * everything else uses split-nibble tables, one class per (element
+//     width, groups); tables that do not fit at once are processed in source
+//     chunks inside the kernel.
+// Work items are (sub-job, part) pairs: part p of P covers the sub-job's
+// column vectors p*T + tid + j*P*T (T threads per CTA), so CTAs holding
+// consecutive items sweep one window of memory together; the remaining parts
+// cover the 4-byte scalar groups of heads, tails and unaligned stripes.
+// Persistent CTAs claim items from an atomic counter and reload their
+// shared-memory tables only when an item needs a different plan. The
+// descriptor blob (jobs, pointers, items, counters) goes to the device in one
+// copy, and a submission whose structure repeats replays a captured graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fgf_cuda.h"
+#include "fast_core.cuh"
+#include "internal.hpp"
+
+namespace fgfc {
+
+namespace {
+
+struct BatchJob {
+  const uint32_t* tables;  // plan compact tables (matrix orientation)
+  uint64_t len;            // bytes per row
+  uint64_t head;           // scalar bytes before the vector body
+  uint64_t nvec;           // 16-byte vectors in the body
+  uint32_t gstride, g0;    // plan groups per (source, plane); first group of this sub-job
+  uint32_t k, nrows;       // sources; rows of this sub-job
+  uint32_t ovr;            // 1 = overwrite
+  uint32_t src_idx, dst_idx;
+  uint32_t nv_items;       // vector items; scalar items follow
+};
+
+constexpr int kThreads = 512;
+constexpr uint32_t kVecPerItem = 8 * kThreads;
+constexpr uint32_t kGroupsPerItem = kThreads;
+constexpr uint32_t kFastVecPerItem = 8 * kFastThreads;
+constexpr uint32_t kFastGroupsPerItem = kFastThreads;
+constexpr uint32_t kClaim = 2;  // items claimed per atomic
+
+// ---------------------------------------------------------------- nibble classes
+
+// Expand compact tables of sources [t0, t0 + kk) into the replicated
+// nibble layout (slot = (t * E + p) * G + g, 4 KiB each), via a staging copy.
+template <int E, int G>
+__device__ void fill_chunk(const BatchJob& J, uint32_t t0, uint32_t kk) {
+  const uint32_t nslots = kk * E * G;
+  uint32_t* stage = reinterpret_cast<uint32_t*>(g_smem) + kMaxSlots * 1024u;
+  __syncthreads();  // previous tables no longer read
+  for (uint32_t i = threadIdx.x; i < nslots * kCompactWords; i += blockDim.x) {
+    const uint32_t slot = i >> 5;
+    const uint32_t tp = t0 * E + slot / G;
+    stage[i] = __ldg(J.tables + (tp * J.gstride + J.g0 + slot % G) * kCompactWords + (i & 31u));
+  }
+  __syncthreads();
+  uint4* st4 = reinterpret_cast<uint4*>(g_smem);
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < nslots * 256u; i += blockDim.x) {
+    const uint32_t v = stage[(i >> 8) * kCompactWords + ((i >> 3) & 1u) * 16u + ((i >> 4) & 15u)];
+    st4[i] = make_uint4(v, v, v, v);
+  }
+  __syncthreads();
+}
+
+template <int E, int G>
+struct Ctx {
+  uint32_t pat;
+  uint32_t lr[E];
+  __device__ __forceinline__ Ctx(uint32_t t, uint32_t lane4) {
+    pat = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) pat |= (((t * E + (b % E)) * G) & 15u) << (8 * b + 4);
+#pragma unroll
+    for (int p = 0; p < E; ++p) lr[p] = lane4 | ((((t * E + p) * G) >> 4) << 16);
+  }
+};
+
+template <int E, int G, int NE>
+__device__ __forceinline__ void fold(uint32_t w, const Ctx<E, G>& c, uint32_t (&acc)[G][NE], int e0) {
+  const uint32_t xl = (w & 0x0F0F0F0Fu) | c.pat;
+  const uint32_t xh = ((w >> 4) & 0x0F0F0F0Fu) | c.pat;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const uint32_t sel = 0x7604u | (static_cast<uint32_t>(b) << 4);
+    const uint32_t al = prmt(xl, c.lr[b % E], sel);
+    const uint32_t ah = prmt(xh, c.lr[b % E], sel);
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      acc[g][e0 + b / E] ^= lds_at(al + g * kSlotBytes) ^ lds_at(ah + g * kSlotBytes + 128);
+  }
+}
+
+template <int E, int G, int NE>
+__device__ __forceinline__ uint32_t out_word(const uint32_t (&acc)[G][NE], int g, int rr, int q) {
+  if (E == 1) {
+    return row_word4(&acc[g][4 * q], rr);
+  } else if (E == 2) {
+    return prmt(acc[g][2 * q], acc[g][2 * q + 1], rr ? 0x7632u : 0x5410u);
+  } else {
+    return acc[g][q];
+  }
+}
+
+// One vector item of a sub-job, for sources [t0, t0 + kk) whose tables are
+// resident; `ovr` overwrites, otherwise the destination is accumulated.
+template <int E, int G>
+__device__ void vector_item(const BatchJob& J, const uint64_t* ptrs, uint32_t part, uint32_t t0,
+                            uint32_t kk, bool ovr) {
+  constexpr int NE = 16 / E, R = 4 / E;
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint64_t step = static_cast<uint64_t>(J.nv_items) * blockDim.x;
+  for (uint64_t v = static_cast<uint64_t>(part) * blockDim.x + threadIdx.x; v < J.nvec; v += step) {
+    const uint64_t off = J.head + v * 16u;
+    uint32_t acc[G][NE];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < NE; ++e) acc[g][e] = 0;
+    const uint8_t* const* srcs = reinterpret_cast<const uint8_t* const*>(ptrs + J.src_idx + t0);
+    uint4 cur = ldg16(srcs[0] + off);
+    for (uint32_t t = 0; t < kk; ++t) {
+      uint4 nxt = cur;
+      if (t + 1 < kk) nxt = ldg16(srcs[t + 1] + off);
+      const Ctx<E, G> c(t, lane4);
+      fold<E, G, NE>(cur.x, c, acc, 0);
+      fold<E, G, NE>(cur.y, c, acc, 4 / E);
+      fold<E, G, NE>(cur.z, c, acc, 2 * (4 / E));
+      fold<E, G, NE>(cur.w, c, acc, 3 * (4 / E));
+      cur = nxt;
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int rr = 0; rr < R; ++rr) {
+        const uint32_t row = g * R + rr;
+        if (row >= J.nrows) continue;
+        uint4 o;
+        o.x = out_word<E, G, NE>(acc, g, rr, 0);
+        o.y = out_word<E, G, NE>(acc, g, rr, 1);
+        o.z = out_word<E, G, NE>(acc, g, rr, 2);
+        o.w = out_word<E, G, NE>(acc, g, rr, 3);
+        uint4* dp = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off);
+        if (!ovr) {
+          const uint4 d = *dp;
+          o.x ^= d.x;
+          o.y ^= d.y;
+          o.z ^= d.z;
+          o.w ^= d.w;
+        }
+        *dp = o;
+      }
+  }
+}
+
+// One scalar item: 4-byte groups of the head [0, head) and the tail
+// [head + 16 * nvec, len) of every row, byte loads and stores.
+template <int E, int G>
+__device__ void scalar_item(const BatchJob& J, const uint64_t* ptrs, uint32_t part, uint32_t t0,
+                            uint32_t kk, bool ovr) {
+  constexpr int R = 4 / E;
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint64_t tail0 = J.head + J.nvec * 16u;
+  const uint64_t n0 = (J.head + 3) / 4, n1 = (J.len - tail0 + 3) / 4;
+  const uint64_t gi = static_cast<uint64_t>(part) * kGroupsPerItem + threadIdx.x;
+  // every thread runs the lookups (uniform control flow); only threads with
+  // a group in range touch memory
+  const bool live = gi < n0 + n1;
+  const uint64_t off = !live ? 0 : (gi < n0 ? 4 * gi : tail0 + 4 * (gi - n0));
+  const uint64_t end = !live ? 0 : (gi < n0 ? J.head : J.len);
+  const int nb = !live ? 0 : static_cast<int>(end - off < 4 ? end - off : 4);
+  uint32_t acc[G][4 / E];
+#pragma unroll
+  for (int g = 0; g < G; ++g)
+#pragma unroll
+    for (int e = 0; e < 4 / E; ++e) acc[g][e] = 0;
+  for (uint32_t t = 0; t < kk; ++t) {
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(ptrs[J.src_idx + t0 + t]) + off;
+    uint32_t w = 0;
+    for (int b = 0; b < nb; ++b) w |= static_cast<uint32_t>(s[b]) << (8 * b);
+    const Ctx<E, G> c(t, lane4);
+    fold<E, G, 4 / E>(w, c, acc, 0);
+  }
+  if (!live) return;
+#pragma unroll
+  for (int g = 0; g < G; ++g)
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const uint32_t row = g * R + rr;
+      if (row >= J.nrows) continue;
+      uint32_t o;
+      if (E == 1) {
+        o = row_word4(&acc[g][0], rr);
+      } else if (E == 2) {
+        o = prmt(acc[g][0], acc[g][1], rr ? 0x7632u : 0x5410u);
+      } else {
+        o = acc[g][0];
+      }
+      uint8_t* d = reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off;
+      for (int b = 0; b < nb; ++b) {
+        const uint8_t v = static_cast<uint8_t>(o >> (8 * b));
+        d[b] = ovr ? v : static_cast<uint8_t>(d[b] ^ v);
+      }
+    }
+}
+
+// Persistent work-list kernel for one nibble (E, G) class.
+template <int E, int G>
+__global__ void __launch_bounds__(kThreads, 1)
+    batch_kernel(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
+                 const uint2* __restrict__ items, uint32_t nitems, uint32_t* counter) {
+  __shared__ uint32_t s_item;
+  __shared__ const uint32_t* s_tab;
+  __shared__ uint32_t s_g0, s_t0;
+  const uint32_t kc = kMaxSlots / (E * G);  // sources whose tables fit at once
+  if (threadIdx.x == 0) {
+    s_tab = nullptr;
+    s_g0 = s_t0 = 0xFFFFFFFFu;
+  }
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, kClaim);
+    __syncthreads();
+    const uint32_t first = s_item;
+    if (first >= nitems) break;
+    for (uint32_t it = first; it < first + kClaim && it < nitems; ++it) {
+      const uint2 wi = items[it];
+      const BatchJob J = jobs[wi.x];
+      const uint32_t nchunks = (J.k + kc - 1) / kc;
+      for (uint32_t c = 0; c < nchunks; ++c) {
+        const uint32_t t0 = c * kc, kk = min(kc, J.k - t0);
+        __syncthreads();
+        const bool resident = s_tab == J.tables && s_g0 == J.g0 && s_t0 == t0;
+        if (!resident) {
+          fill_chunk<E, G>(J, t0, kk);
+          if (threadIdx.x == 0) {
+            s_tab = J.tables;
+            s_g0 = J.g0;
+            s_t0 = t0;
+          }
+        }
+        const bool ovr = J.ovr && c == 0;
+        if (wi.y < J.nv_items)
+          vector_item<E, G>(J, ptrs, wi.y, t0, kk, ovr);
+        else
+          scalar_item<E, G>(J, ptrs, wi.y - J.nv_items, t0, kk, ovr);
+        __syncthreads();  // chunk c's writes precede chunk c + 1's reads of the same rows
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- byte-table classes
+
+// Work-list kernel for Gf8 sub-jobs of at most 4 rows and exactly K sources.
+// The plan's tables stay resident across consecutive items of one plan.
+template <int K>
+__global__ void __launch_bounds__(kFastThreads, 1)
+    batch_fast_kernel(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
+                      const uint2* __restrict__ items, uint32_t nitems, uint32_t* counter) {
+  __shared__ uint32_t s_item;
+  __shared__ const uint32_t* s_tab;
+  __shared__ uint32_t s_g0;
+  __shared__ const uint8_t* s_src[K];
+  __shared__ uint8_t* s_dst[4];
+  if (threadIdx.x == 0) {
+    s_tab = nullptr;
+    s_g0 = 0xFFFFFFFFu;
+  }
+  const FastRegs r;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, kClaim);
+    __syncthreads();
+    const uint32_t first = s_item;
+    if (first >= nitems) break;
+    for (uint32_t it = first; it < first + kClaim && it < nitems; ++it) {
+      const uint2 wi = items[it];
+      const BatchJob J = jobs[wi.x];
+      __syncthreads();  // the previous item is done with tables and pointers
+      const bool resident = s_tab == J.tables && s_g0 == J.g0;
+      if (threadIdx.x < K) s_src[threadIdx.x] = reinterpret_cast<const uint8_t*>(ptrs[J.src_idx + threadIdx.x]);
+      if (threadIdx.x < J.nrows) s_dst[threadIdx.x] = reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + threadIdx.x]);
+      if (!resident) {
+        fill_fast<K>(J.tables, nullptr, J.gstride, J.g0);
+        if (threadIdx.x == 0) {
+          s_tab = J.tables;
+          s_g0 = J.g0;
+        }
+      }
+      __syncthreads();
+      const bool ovr = J.ovr != 0;
+      if (wi.y < J.nv_items) {
+        const uint64_t step = static_cast<uint64_t>(J.nv_items) * blockDim.x;
+        for (uint64_t v = static_cast<uint64_t>(wi.y) * blockDim.x + threadIdx.x; v < J.nvec; v += step) {
+          const uint64_t off = J.head + v * 16u;
+          uint32_t w[K][4];
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            const uint4 x = ldg16(s_src[t] + off);
+            w[t][0] = x.x;
+            w[t][1] = x.y;
+            w[t][2] = x.z;
+            w[t][3] = x.w;
+          }
+          uint32_t acc[16];
+#pragma unroll
+          for (int e = 0; e < 16; ++e) acc[e] = 0;
+          fast_fold<K, 4>(w, acc, r);
+          store_col4(acc, s_dst, J.nrows, off, ovr);
+        }
+      } else {
+        const uint64_t tail0 = J.head + J.nvec * 16u;
+        const uint64_t n0 = (J.head + 3) / 4, n1 = (J.len - tail0 + 3) / 4;
+        const uint64_t gi = static_cast<uint64_t>(wi.y - J.nv_items) * kFastGroupsPerItem + threadIdx.x;
+        if (gi < n0 + n1) {
+          const uint64_t off = gi < n0 ? 4 * gi : tail0 + 4 * (gi - n0);
+          const uint64_t end = gi < n0 ? J.head : J.len;
+          const int nb = static_cast<int>(end - off < 4 ? end - off : 4);
+          uint32_t w[K][1];
+#pragma unroll
+          for (int t = 0; t < K; ++t) {
+            uint32_t x = 0;
+            for (int b = 0; b < nb; ++b) x |= static_cast<uint32_t>(s_src[t][off + b]) << (8 * b);
+            w[t][0] = x;
+          }
+          uint32_t acc[4] = {0, 0, 0, 0};
+          fast_fold<K, 1>(w, acc, r);
+          for (uint32_t rr = 0; rr < J.nrows; ++rr) {
+            const uint32_t o = row_word4(acc, static_cast<int>(rr));
+            uint8_t* d = s_dst[rr] + off;
+            for (int b = 0; b < nb; ++b) {
+              const uint8_t v = static_cast<uint8_t>(o >> (8 * b));
+              d[b] = ovr ? v : static_cast<uint8_t>(d[b] ^ v);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// Uniform-plan variant: every sub-job of the class shares one plan, so each
+// CTA loads the tables once and grid-strides over the flattened column space
+// of all sub-jobs (vector columns first, then scalar groups), exactly like one
+// long call. The per-stripe pointers and geometry travel in the launch
+// parameters (constant bank), so the per-column job lookup is a few cached
+// constant loads instead of a chain of dependent global loads; a class with
+// more stripes than one parameter block holds is split into launches.
+constexpr int kUniformJobs = 160;
+
+struct UJob {
+  const uint8_t* src[kFastMaxK];
+  uint8_t* dst[4];
+  uint64_t len, head, nvec;
+  uint32_t nrows, ovr;
+};
+
+struct UniformParams {
+  const uint32_t* tables;
+  uint32_t gstride, g0, njobs, pad;
+  uint64_t vprefix[kUniformJobs + 1];
+  uint64_t gprefix[kUniformJobs + 1];
+  UJob jobs[kUniformJobs];
+};
+static_assert(sizeof(UniformParams) <= 32000, "launch parameter block too large");
+
+template <int K>
+__global__ void __launch_bounds__(kFastThreads, 1)
+    batch_fast_uniform_kernel(const __grid_constant__ UniformParams P) {
+  fill_fast<K>(P.tables, nullptr, P.gstride, P.g0);
+  const FastRegs r;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t vtotal = P.vprefix[P.njobs];
+  uint32_t j = 0;
+  for (uint64_t u = tid; u < vtotal; u += stride) {
+    while (u >= P.vprefix[j + 1]) ++j;
+    const UJob& J = P.jobs[j];
+    const uint64_t off = J.head + (u - P.vprefix[j]) * 16u;
+    uint32_t w[K][4];
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      const uint4 x = ldg16(J.src[t] + off);
+      w[t][0] = x.x;
+      w[t][1] = x.y;
+      w[t][2] = x.z;
+      w[t][3] = x.w;
+    }
+    uint32_t acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0;
+    fast_fold<K, 4>(w, acc, r);
+    store_col4(acc, J.dst, J.nrows, off, J.ovr != 0);
+  }
+  const uint64_t gtotal = P.gprefix[P.njobs];
+  j = 0;
+  for (uint64_t u = tid; u < gtotal; u += stride) {
+    while (u >= P.gprefix[j + 1]) ++j;
+    const UJob& J = P.jobs[j];
+    const uint64_t gi = u - P.gprefix[j];
+    const uint64_t tail0 = J.head + J.nvec * 16u;
+    const uint64_t n0 = (J.head + 3) / 4;
+    const uint64_t off = gi < n0 ? 4 * gi : tail0 + 4 * (gi - n0);
+    const uint64_t end = gi < n0 ? J.head : J.len;
+    const int nb = static_cast<int>(end - off < 4 ? end - off : 4);
+    uint32_t w[K][1];
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+      uint32_t x = 0;
+      for (int bb = 0; bb < nb; ++bb) x |= static_cast<uint32_t>(J.src[t][off + bb]) << (8 * bb);
+      w[t][0] = x;
+    }
+    uint32_t acc[4] = {0, 0, 0, 0};
+    fast_fold<K, 1>(w, acc, r);
+    for (uint32_t rr = 0; rr < J.nrows; ++rr) {
+      const uint32_t o = row_word4(acc, static_cast<int>(rr));
+      uint8_t* d = J.dst[rr] + off;
+      for (int bb = 0; bb < nb; ++bb) {
+        const uint8_t v = static_cast<uint8_t>(o >> (8 * bb));
+        d[bb] = J.ovr ? v : static_cast<uint8_t>(d[bb] ^ v);
+      }
+    }
+  }
+}
+
+using KernelFn = void (*)(const BatchJob*, const uint64_t*, const uint2*, uint32_t, uint32_t*);
+using UniformFn = void (*)(UniformParams);
+
+KernelFn kernel_for(int E, int G) {
+  switch (E * 8 + G) {
+    case 8 + 1: return batch_kernel<1, 1>;
+    case 8 + 2: return batch_kernel<1, 2>;
+    case 8 + 3: return batch_kernel<1, 3>;
+    case 8 + 4: return batch_kernel<1, 4>;
+    case 16 + 1: return batch_kernel<2, 1>;
+    case 16 + 2: return batch_kernel<2, 2>;
+    case 16 + 3: return batch_kernel<2, 3>;
+    case 16 + 4: return batch_kernel<2, 4>;
+    case 32 + 1: return batch_kernel<4, 1>;
+    case 32 + 2: return batch_kernel<4, 2>;
+    case 32 + 3: return batch_kernel<4, 3>;
+    case 32 + 4: return batch_kernel<4, 4>;
+    default: return nullptr;
+  }
+}
+
+#define FGFC_K_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
+
+KernelFn fast_kernel_for(int K) {
+  switch (K) {
+#define FGFC_CASE(k) \
+  case k: return batch_fast_kernel<k>;
+    FGFC_K_CASES(FGFC_CASE)
+#undef FGFC_CASE
+    default: return nullptr;
+  }
+}
+
+UniformFn uniform_kernel_for(int K) {
+  switch (K) {
+#define FGFC_CASE(k) \
+  case k: return batch_fast_uniform_kernel<k>;
+    FGFC_K_CASES(FGFC_CASE)
+#undef FGFC_CASE
+    default: return nullptr;
+  }
+}
+
+uint32_t fast_smem(int K) {
+  switch (K) {
+#define FGFC_CASE(k) \
+  case k: return FastLayout<k>::smem;
+    FGFC_K_CASES(FGFC_CASE)
+#undef FGFC_CASE
+    default: return 0;
+  }
+}
+
+constexpr size_t kBatchSmem = kMaxSlots * (kSlotBytes + kCompactWords * 4);
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+
+struct BatchClass {
+  int E, G;
+  int K = 0;                   // > 0: byte-table class of Gf8 sub-jobs with K sources
+  std::vector<uint32_t> jobs;  // sub-job indices, plan order
+  std::vector<uint2> items;
+  bool uniform = false;        // byte-table class whose sub-jobs share one plan
+};
+
+struct BatchSlot {
+  uint8_t* host = nullptr;  // pinned
+  uint8_t* dev = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;  // the last submission out of this slot finished
+  cudaGraphExec_t graph = nullptr;
+  std::string key;
+};
+
+struct BatchState {
+  std::vector<UniformParams> uparams;
+  BatchSlot slot[2];
+  int next = 0;
+  bool graphs = true;
+  cudaStream_t capture = nullptr;
+  size_t last_launches = 0, last_items = 0;
+  int last_replayed = 0;
+  std::mutex mu;
+};
+
+static cudaError_t ensure_slot(BatchSlot& s, size_t bytes) {
+  if (s.cap >= bytes) return cudaSuccess;
+  if (s.host) cudaFreeHost(s.host);
+  if (s.dev) cudaFree(s.dev);
+  s.host = nullptr;
+  s.dev = nullptr;
+  if (s.graph) {
+    cudaGraphExecDestroy(s.graph);
+    s.graph = nullptr;
+  }
+  s.key.clear();
+  size_t cap = 1 << 16;
+  while (cap < bytes) cap <<= 1;
+  cudaError_t e = cudaHostAlloc(&s.host, cap, cudaHostAllocDefault);
+  if (e != cudaSuccess) return e;
+  e = cudaMalloc(&s.dev, cap);
+  if (e != cudaSuccess) return e;
+  if (!s.done) {
+    e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  s.cap = cap;
+  return cudaSuccess;
+}
+
+void* batch_state_create() { return new BatchState(); }
+
+void batch_state_destroy(void* p) {
+  BatchState* b = static_cast<BatchState*>(p);
+  if (!b) return;
+  for (auto& s : b->slot) {
+    if (s.done) cudaEventSynchronize(s.done);
+    if (s.graph) cudaGraphExecDestroy(s.graph);
+    if (s.host) cudaFreeHost(s.host);
+    if (s.dev) cudaFree(s.dev);
+    if (s.done) cudaEventDestroy(s.done);
+  }
+  if (b->capture) cudaStreamDestroy(b->capture);
+  delete b;
+}
+
+void batch_state_graphs(void* p, bool on) { static_cast<BatchState*>(p)->graphs = on; }
+
+void batch_state_stats(const void* p, size_t* launches, size_t* items, int* replayed) {
+  const BatchState* b = static_cast<const BatchState*>(p);
+  if (launches) *launches = b->last_launches;
+  if (items) *items = b->last_items;
+  if (replayed) *replayed = b->last_replayed;
+}
+
+static size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+
+cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream) {
+  BatchState* b = static_cast<BatchState*>(state);
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->last_launches = b->last_items = 0;
+  b->last_replayed = 0;
+  if (jobs.empty()) return cudaSuccess;
+
+  // ---- device descriptors, pointer array, classes (sub-jobs in plan order)
+  std::vector<BatchJob> dj(jobs.size());
+  std::vector<uint64_t> ptrs;
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const LoweredJob& L = jobs[i];
+    BatchJob& J = dj[i];
+    J.tables = L.tables;
+    J.len = L.len;
+    J.head = L.head;
+    J.nvec = L.nvec;
+    J.gstride = static_cast<uint32_t>(L.gstride);
+    J.g0 = static_cast<uint32_t>(L.g0);
+    J.k = static_cast<uint32_t>(L.k);
+    J.nrows = static_cast<uint32_t>(L.nrows);
+    J.ovr = L.ovr ? 1u : 0u;
+    J.src_idx = static_cast<uint32_t>(ptrs.size());
+    ptrs.insert(ptrs.end(), L.srcs.begin(), L.srcs.end());
+    J.dst_idx = static_cast<uint32_t>(ptrs.size());
+    ptrs.insert(ptrs.end(), L.dsts.begin(), L.dsts.end());
+    J.nv_items = 0;
+  }
+  std::vector<size_t> order(jobs.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) {
+    return jobs[a].tables != jobs[c].tables ? jobs[a].tables < jobs[c].tables : jobs[a].g0 < jobs[c].g0;
+  });
+  std::map<int, BatchClass> classes;  // key E * 8 + G, or 100 + K for byte-table classes
+  for (size_t i : order) {
+    const LoweredJob& L = jobs[i];
+    const int E = field_bytes(L.field);
+    const bool fast = E == 1 && L.G == 1 && L.k >= 1 && L.k <= static_cast<size_t>(kFastMaxK);
+    const int key = fast ? 100 + static_cast<int>(L.k) : E * 8 + static_cast<int>(L.G);
+    BatchClass& c = classes[key];
+    c.E = E;
+    c.G = static_cast<int>(L.G);
+    c.K = fast ? static_cast<int>(L.k) : 0;
+    c.jobs.push_back(static_cast<uint32_t>(i));
+  }
+  for (auto& kv : classes) {
+    BatchClass& c = kv.second;
+    c.uniform = c.K > 0;
+    for (uint32_t i : c.jobs)
+      c.uniform = c.uniform && jobs[i].tables == jobs[c.jobs[0]].tables && jobs[i].g0 == jobs[c.jobs[0]].g0;
+    if (c.uniform) continue;
+    const uint64_t per_vec = c.K ? kFastVecPerItem : kVecPerItem;
+    const uint64_t per_grp = c.K ? kFastGroupsPerItem : kGroupsPerItem;
+    for (uint32_t i : c.jobs) {
+      const LoweredJob& L = jobs[i];
+      const uint64_t nv_items = (L.nvec + per_vec - 1) / per_vec;
+      const uint64_t tail = L.len - L.head - 16 * L.nvec;
+      const uint64_t ngroups = (L.head + 3) / 4 + (tail + 3) / 4;
+      const uint64_t ns_items = (ngroups + per_grp - 1) / per_grp;
+      dj[i].nv_items = static_cast<uint32_t>(nv_items);
+      for (uint64_t p = 0; p < nv_items + ns_items; ++p) c.items.push_back(make_uint2(i, static_cast<unsigned>(p)));
+    }
+  }
+
+  // ---- blob: jobs | ptrs | per work-list class: items, counter
+  size_t off = 0;
+  const size_t off_jobs = off;
+  off = align16(off + dj.size() * sizeof(BatchJob));
+  const size_t off_ptrs = off;
+  off = align16(off + ptrs.size() * sizeof(uint64_t));
+  std::vector<std::pair<size_t, size_t>> cb;  // (items, counter) offsets
+  for (auto& kv : classes) {
+    std::pair<size_t, size_t> x{0, 0};
+    if (!kv.second.uniform) {
+      x.first = off;
+      off = align16(off + kv.second.items.size() * sizeof(uint2));
+      x.second = off;
+      off = align16(off + 64);
+    }
+    cb.push_back(x);
+  }
+  const size_t bytes = off;
+
+  BatchSlot& s = b->slot[b->next];
+  b->next ^= 1;
+  cudaError_t e = cudaSuccess;
+  if (s.done) {
+    e = cudaEventSynchronize(s.done);  // the previous submission out of this slot finished
+    if (e != cudaSuccess) return e;
+  }
+  e = ensure_slot(s, bytes);
+  if (e != cudaSuccess) return e;
+  std::memcpy(s.host + off_jobs, dj.data(), dj.size() * sizeof(BatchJob));
+  std::memcpy(s.host + off_ptrs, ptrs.data(), ptrs.size() * sizeof(uint64_t));
+  {
+    size_t ci = 0;
+    for (auto& kv : classes) {
+      const auto& x = cb[ci++];
+      if (kv.second.uniform) continue;
+      std::memcpy(s.host + x.first, kv.second.items.data(), kv.second.items.size() * sizeof(uint2));
+      std::memset(s.host + x.second, 0, 64);
+    }
+  }
+
+  // ---- launches (their structure is the graph key)
+  struct Launch {
+    KernelFn fn = nullptr;
+    UniformFn ufn = nullptr;
+    unsigned grid = 0, threads = 0;
+    uint32_t smem = 0;
+    const uint2* items = nullptr;
+    uint32_t n = 0;
+    uint32_t* counter = nullptr;
+    size_t uparam = 0;
+  };
+  std::vector<Launch> launches;
+  std::vector<UniformParams>& uparams = b->uparams;
+  uparams.clear();
+  std::string key = std::to_string(reinterpret_cast<uintptr_t>(s.dev)) + ":" + std::to_string(bytes);
+  const int sms = sm_count();
+  static std::mutex attr_mu;
+  static bool attr_set[256] = {false};
+  size_t ci = 0;
+  for (auto& kv : classes) {
+    const BatchClass& c = kv.second;
+    const auto& x = cb[ci++];
+    const bool fast = c.K > 0;
+    Launch L;
+    const int akey = kv.first + (c.uniform ? 100 : 0);
+    if (c.uniform) {
+      L.ufn = uniform_kernel_for(c.K);
+    } else {
+      L.fn = fast ? fast_kernel_for(c.K) : kernel_for(c.E, c.G);
+    }
+    if (!L.fn && !L.ufn) return cudaErrorInvalidValue;
+    L.smem = fast ? fast_smem(c.K) : static_cast<uint32_t>(kBatchSmem);
+    L.threads = fast ? static_cast<unsigned>(kFastThreads) : static_cast<unsigned>(kThreads);
+    {
+      std::lock_guard<std::mutex> lk2(attr_mu);
+      if (!attr_set[akey]) {
+        e = L.ufn ? cudaFuncSetAttribute(L.ufn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.smem))
+                  : cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.smem));
+        if (e != cudaSuccess) return e;
+        attr_set[akey] = true;
+      }
+    }
+    if (c.uniform) {
+      // one launch per block of kUniformJobs stripes
+      for (size_t q0 = 0; q0 < c.jobs.size(); q0 += kUniformJobs) {
+        const size_t nq = std::min<size_t>(kUniformJobs, c.jobs.size() - q0);
+        uparams.emplace_back();
+        UniformParams& P = uparams.back();
+        std::memset(&P, 0, sizeof P);
+        const BatchJob& J0 = dj[c.jobs[q0]];
+        P.tables = J0.tables;
+        P.gstride = J0.gstride;
+        P.g0 = J0.g0;
+        P.njobs = static_cast<uint32_t>(nq);
+        for (size_t q = 0; q < nq; ++q) {
+          const LoweredJob& LJ = jobs[c.jobs[q0 + q]];
+          UJob& U = P.jobs[q];
+          for (size_t t = 0; t < LJ.k; ++t) U.src[t] = reinterpret_cast<const uint8_t*>(LJ.srcs[t]);
+          for (size_t rr = 0; rr < 4; ++rr) U.dst[rr] = reinterpret_cast<uint8_t*>(LJ.dsts[rr < LJ.nrows ? rr : 0]);
+          U.len = LJ.len;
+          U.head = LJ.head;
+          U.nvec = LJ.nvec;
+          U.nrows = static_cast<uint32_t>(LJ.nrows);
+          U.ovr = LJ.ovr ? 1u : 0u;
+          const uint64_t tail = LJ.len - LJ.head - 16 * LJ.nvec;
+          P.vprefix[q + 1] = P.vprefix[q] + LJ.nvec;
+          P.gprefix[q + 1] = P.gprefix[q] + (LJ.head + 3) / 4 + (tail + 3) / 4;
+        }
+        Launch U = L;
+        const uint64_t want = (std::max(P.vprefix[nq], P.gprefix[nq]) + L.threads - 1) / L.threads;
+        U.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(want, sms)));
+        U.uparam = uparams.size() - 1;
+        // the parameter block is baked into a captured graph: hash it into the key
+        uint64_t h = 1469598103934665603ull;
+        const uint8_t* pb = reinterpret_cast<const uint8_t*>(&P);
+        for (size_t i = 0; i < sizeof P; ++i) h = (h ^ pb[i]) * 1099511628211ull;
+        key += "|u" + std::to_string(akey) + "," + std::to_string(h) + "," + std::to_string(U.grid);
+        launches.push_back(U);
+      }
+      b->last_items += c.jobs.size();
+    } else {
+      L.n = static_cast<uint32_t>(c.items.size());
+      L.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((L.n + kClaim - 1) / kClaim, sms)));
+      L.items = reinterpret_cast<const uint2*>(s.dev + x.first);
+      L.counter = reinterpret_cast<uint32_t*>(s.dev + x.second);
+      b->last_items += c.items.size();
+      key += "|" + std::to_string(akey) + "," + std::to_string(L.n) + "," + std::to_string(L.grid);
+      launches.push_back(L);
+    }
+  }
+  const BatchJob* djobs = reinterpret_cast<const BatchJob*>(s.dev + off_jobs);
+  const uint64_t* dptrs = reinterpret_cast<const uint64_t*>(s.dev + off_ptrs);
+
+  auto enqueue = [&](cudaStream_t st) -> cudaError_t {
+    cudaError_t err = cudaMemcpyAsync(s.dev, s.host, bytes, cudaMemcpyHostToDevice, st);
+    if (err != cudaSuccess) return err;
+    for (const Launch& L : launches) {
+      if (L.ufn)
+        L.ufn<<<L.grid, L.threads, L.smem, st>>>(uparams[L.uparam]);
+      else
+        L.fn<<<L.grid, L.threads, L.smem, st>>>(djobs, dptrs, L.items, L.n, L.counter);
+      err = cudaGetLastError();
+      if (err != cudaSuccess) return err;
+    }
+    return cudaSuccess;
+  };
+
+  b->last_launches = launches.size();
+  if (b->graphs) {
+    if (!(s.graph && s.key == key)) {
+      if (s.graph) {
+        cudaGraphExecDestroy(s.graph);
+        s.graph = nullptr;
+      }
+      if (!b->capture) {
+        e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+      }
+      cudaGraph_t g = nullptr;
+      e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return e;
+      const cudaError_t ee = enqueue(b->capture);
+      e = cudaStreamEndCapture(b->capture, &g);
+      if (ee != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ee;
+      }
+      if (e != cudaSuccess) return e;
+      e = cudaGraphInstantiate(&s.graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        s.graph = nullptr;
+        return e;
+      }
+      s.key = key;
+    } else {
+      b->last_replayed = 1;
+    }
+    e = cudaGraphLaunch(s.graph, stream);
+  } else {
+    e = enqueue(stream);
+  }
+  if (e != cudaSuccess) return e;
+  return cudaEventRecord(s.done, stream);
+}
+
+}  // namespace fgfc

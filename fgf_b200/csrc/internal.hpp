@@ -63,4 +63,24 @@ cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const 
 
 int sm_count();
 
+// One lowered sub-job of a batched submission: all sources of a stripe and
+// the rows of at most 4 table groups, with its alignment split resolved.
+struct LoweredJob {
+  int field;
+  const uint32_t* tables;  // plan compact tables, matrix orientation
+  size_t gstride;          // plan groups per (source, plane)
+  size_t g0;               // first group of this sub-job
+  size_t G;                // groups in this sub-job (1..4)
+  uint64_t len, head, nvec;
+  size_t k, nrows;
+  bool ovr;
+  std::vector<uint64_t> srcs, dsts;
+};
+
+void* batch_state_create();
+void batch_state_destroy(void* state);
+void batch_state_graphs(void* state, bool on);
+void batch_state_stats(const void* state, size_t* launches, size_t* items, int* replayed);
+cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream);
+
 }  // namespace fgfc

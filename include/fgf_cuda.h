@@ -195,6 +195,46 @@ fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t *dst, size_t dst_len, siz
                                                const fgfc_plan *plan, const fgfc_slice *srcs,
                                                size_t nsrcs, fgfc_stream stream);
 
+/* ---------------------------------------------------------------- batches */
+
+/* One stripe of a batched submission: the arguments of one
+ * dot_product_matrix_with (overwrite = 1), mul_add_matrix_with (overwrite =
+ * 0, row_starts = NULL) or mul_add_matrix_scattered_with (row_starts set)
+ * call (src/ops.rs:720-867, 887-941). Each job is validated exactly as that
+ * call would be. */
+typedef struct fgfc_matrix_job {
+  const fgfc_plan *plan;    /* dimensions (nsrcs, nrows) */
+  const fgfc_slice *srcs;   /* host array of nsrcs device slices */
+  size_t nsrcs;
+  uint8_t *dst;             /* device destination base */
+  size_t dst_len;
+  const size_t *row_starts; /* host array of nrows offsets into dst, or NULL for rows j * row_len */
+  size_t nrows;
+  size_t row_len;
+  int overwrite;
+} fgfc_matrix_job;
+
+/* A reusable batch runner. No reference counterpart: the reference is a
+ * single-threaded CPU library that serves one call at a time. The runner
+ * owns its device work-list and pinned staging (grown on demand, reused
+ * afterwards) and lowers every submission to one persistent launch per
+ * (element width, row-group) class. */
+typedef struct fgfc_batch fgfc_batch;
+
+fgfc_status fgfc_batch_create(fgfc_batch **out);
+void fgfc_batch_destroy(fgfc_batch *batch);
+/* Replay submissions whose launch structure repeats as a captured CUDA graph
+ * (default on). */
+fgfc_status fgfc_batch_set_graphs(fgfc_batch *batch, int enable);
+/* Enqueue all jobs on `stream`. Jobs must not write memory another job of the
+ * same submission reads or writes. */
+fgfc_status fgfc_batch_run(fgfc_batch *batch, const fgfc_matrix_job *jobs, size_t njobs,
+                           fgfc_stream stream);
+/* Statistics of the last submission: kernel launches issued, work items,
+ * whether it replayed a graph. */
+fgfc_status fgfc_batch_stats(const fgfc_batch *batch, size_t *launches, size_t *items,
+                             int *graph_replayed);
+
 #ifdef __cplusplus
 }
 #endif
