@@ -47,6 +47,22 @@ class MatrixJob(C.Structure):
     ]
 
 
+class NoAllocJob(C.Structure):
+    """fgfc_noalloc_job: one stripe of fgfc_batch_run_noalloc (raw coefficients)."""
+
+    _fields_ = [
+        ("coeffs", C.POINTER(C.c_uint32)),
+        ("srcs", C.POINTER(Slice)),
+        ("nsrcs", C.c_size_t),
+        ("dst", C.c_void_p),
+        ("dst_len", C.c_size_t),
+        ("row_starts", C.POINTER(C.c_size_t)),
+        ("nrows", C.c_size_t),
+        ("row_len", C.c_size_t),
+        ("overwrite", C.c_int),
+    ]
+
+
 _SIGS = {
     "fgfc_last_error": (C.c_char_p, []),
     "fgfc_version": (C.c_char_p, []),
@@ -94,6 +110,7 @@ _SIGS = {
     "fgfc_batch_set_graphs": (c_status, [C.c_void_p, C.c_int]),
     "fgfc_batch_run": (c_status, [C.c_void_p, C.POINTER(MatrixJob), c_size, c_stream]),
     "fgfc_batch_stats": (c_status, [C.c_void_p, C.POINTER(c_size), C.POINTER(c_size), C.POINTER(C.c_int)]),
+    "fgfc_batch_run_noalloc": (c_status, [C.c_int, C.POINTER(NoAllocJob), c_size, c_stream]),
 }
 
 _lib: C.CDLL | None = None

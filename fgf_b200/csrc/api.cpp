@@ -918,4 +918,46 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
   return e == cudaSuccess ? ok() : cuda_fail(e, "batch");
 }
 
+// Same per-job rules as fgfc_batch_run, with the raw coefficient forms'
+// names; the limits of the fixed scratch are checked by noalloc_run before
+// anything is issued. Nothing is allocated on success.
+fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job* jobs, size_t njobs,
+                                   fgfc_stream stream) {
+  if (!valid_field(field) || (njobs && !jobs)) return fail(FGFC_ERR_ARG, "batch_run_noalloc: invalid argument");
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_noalloc_job& J = jobs[i];
+    const char* name =
+        J.row_starts ? "mul_add_matrix_scattered" : (J.overwrite ? "dot_product_matrix" : "mul_add_matrix");
+    fgfc_status st;
+    if (J.row_starts) {
+      if (J.overwrite)
+        return fail(FGFC_ERR_ARG, "batch job %zu: scattered rows accumulate; overwrite is not defined", i);
+      if (!check_scattered_rows(field, name, J.dst_len, J.row_len, J.row_starts, J.nrows, &st)) {
+        t_err = "batch job " + std::to_string(i) + ": " + t_err;
+        return st;
+      }
+    } else {
+      if (!check_width(field, name, J.row_len, &st)) {
+        t_err = "batch job " + std::to_string(i) + ": " + t_err;
+        return st;
+      }
+      size_t used;
+      if (mul_overflows(J.nrows, J.row_len, &used))
+        return fail(FGFC_ERR_OVERFLOW, "batch job %zu: %s: row geometry overflows", i, name);
+      if (J.dst_len < used)
+        return fail(FGFC_ERR_ROWS, "batch job %zu: %s: rows is %zu bytes but %zu rows of %zu bytes need %zu",
+                    i, name, J.dst_len, J.nrows, J.row_len, used);
+    }
+    if (J.nsrcs && !J.srcs) return fail(FGFC_ERR_ARG, "batch job %zu: %s: null sources", i, name);
+    if (J.nsrcs && J.nrows && !J.coeffs) return fail(FGFC_ERR_ARG, "batch job %zu: %s: null coefficients", i, name);
+    for (size_t t = 0; t < J.nsrcs; ++t)
+      if (J.srcs[t].len != J.row_len)
+        return fail(FGFC_ERR_SOURCE, "batch job %zu: %s: source %zu is %zu bytes, expected %zu", i, name, t,
+                    J.srcs[t].len, J.row_len);
+  }
+  char msg[256];
+  const int st = noalloc_run(field, jobs, njobs, stream, msg, sizeof msg);
+  return st == 0 ? ok() : fail(static_cast<fgfc_status>(st), "%s", msg);
+}
+
 }  // extern "C"

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -829,6 +830,164 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   }
   if (e != cudaSuccess) return e;
   return cudaEventRecord(s.done, stream);
+}
+
+// ---------------------------------------------------------------- without allocation
+//
+// fgfc_batch_run_noalloc: the work-list kernel above, with every byte of
+// scratch it needs (descriptors, pointers, work items, the claim counter and
+// the stripes' compact product tables) placed in this fixed device array
+// instead of device memory allocated for the call. The host side builds the
+// whole blob in a fixed host array of the same size and copies it in with one
+// stream-ordered copy, so nothing is allocated on either side.
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[FGFC_NOALLOC_SCRATCH_BYTES];
+alignas(256) static uint8_t g_noalloc_host[FGFC_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mu;
+constexpr int kNoallocMaxDevices = 64;
+static uint8_t* g_noalloc_dev[kNoallocMaxDevices];  // device address of the array, per device
+
+// Returns 0, or an fgfc_status-style code with `msg` filled in.
+int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStream_t stream, char* msg,
+                size_t msglen) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+    snprintf(msg, msglen, "batch_run_noalloc: no usable current device");
+    return FGFC_ERR_CUDA;
+  }
+  if (!g_noalloc_dev[dev]) {
+    // The array's name is only a host-side stand-in; the kernels need its
+    // device address on this device.
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      snprintf(msg, msglen, "batch_run_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return FGFC_ERR_CUDA;
+    }
+    g_noalloc_dev[dev] = static_cast<uint8_t*>(p);
+  }
+  uint8_t* const dbase = g_noalloc_dev[dev];
+  const int E = field_bytes(field);
+  const int R = 4 / E;
+
+  // ---- sizes (one class: every stripe uses G table groups)
+  size_t G = 1, nptr = 0, ntab = 0, nitems = 0, nlive = 0;
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_noalloc_job& J = jobs[i];
+    if (J.nrows == 0 || J.row_len == 0 || J.nsrcs == 0) continue;
+    if (J.nrows > static_cast<size_t>(4 * R) || J.nsrcs > static_cast<size_t>(kMaxSrc)) {
+      snprintf(msg, msglen, "batch_run_noalloc: job %zu has %zu rows and %zu sources; at most %d rows and %d sources",
+               i, J.nrows, J.nsrcs, 4 * R, kMaxSrc);
+      return FGFC_ERR_LIMIT;
+    }
+    G = std::max<size_t>(G, (J.nrows + R - 1) / R);
+  }
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_noalloc_job& J = jobs[i];
+    if (J.nrows == 0 || J.row_len == 0 || J.nsrcs == 0) continue;
+    ++nlive;
+    nptr += J.nsrcs + J.nrows;
+    ntab += J.nsrcs * E * G * kCompactWords;
+    const uint64_t nvec = J.row_len / 16 + 1;  // upper bound before alignment is known
+    nitems += (nvec + kVecPerItem - 1) / kVecPerItem + (J.row_len / 4 + 2 + kGroupsPerItem - 1) / kGroupsPerItem + 1;
+  }
+  const size_t off_jobs = 0;
+  const size_t off_ptrs = align16(off_jobs + nlive * sizeof(BatchJob));
+  const size_t off_tabs = align16(off_ptrs + nptr * sizeof(uint64_t));
+  const size_t off_items = align16(off_tabs + ntab * sizeof(uint32_t));
+  const size_t off_counter = align16(off_items + nitems * sizeof(uint2));
+  const size_t bytes = off_counter + 64;
+  if (bytes > FGFC_NOALLOC_SCRATCH_BYTES) {
+    snprintf(msg, msglen, "batch_run_noalloc: submission needs %zu bytes of scratch, more than the %u available",
+             bytes, static_cast<unsigned>(FGFC_NOALLOC_SCRATCH_BYTES));
+    return FGFC_ERR_LIMIT;
+  }
+
+  // ---- blob in the host array
+  BatchJob* hj = reinterpret_cast<BatchJob*>(g_noalloc_host + off_jobs);
+  uint64_t* hp = reinterpret_cast<uint64_t*>(g_noalloc_host + off_ptrs);
+  uint32_t* ht = reinterpret_cast<uint32_t*>(g_noalloc_host + off_tabs);
+  uint2* hi = reinterpret_cast<uint2*>(g_noalloc_host + off_items);
+  size_t jn = 0, pn = 0, tn = 0, in = 0;
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_noalloc_job& S = jobs[i];
+    if (S.nrows == 0 || S.row_len == 0) continue;
+    if (S.nsrcs == 0) {
+      if (S.overwrite) {  // an empty sum overwrites with zero
+        for (size_t j = 0; j < S.nrows; ++j) {
+          e = cudaMemsetAsync(S.dst + (S.row_starts ? S.row_starts[j] : j * S.row_len), 0, S.row_len, stream);
+          if (e != cudaSuccess) {
+            snprintf(msg, msglen, "batch_run_noalloc: %s", cudaGetErrorString(e));
+            return FGFC_ERR_CUDA;
+          }
+        }
+      }
+      continue;
+    }
+    BatchJob& J = hj[jn];
+    const uintptr_t al = reinterpret_cast<uintptr_t>(S.srcs[0].ptr) & 15;
+    bool same = (al % E) == 0;
+    J.src_idx = static_cast<uint32_t>(pn);
+    for (size_t t = 0; t < S.nsrcs; ++t) {
+      hp[pn] = reinterpret_cast<uint64_t>(S.srcs[t].ptr);
+      same = same && (hp[pn] & 15) == al;
+      ++pn;
+    }
+    J.dst_idx = static_cast<uint32_t>(pn);
+    for (size_t j = 0; j < S.nrows; ++j) {
+      hp[pn] = reinterpret_cast<uint64_t>(S.dst + (S.row_starts ? S.row_starts[j] : j * S.row_len));
+      same = same && (hp[pn] & 15) == al;
+      ++pn;
+    }
+    J.len = S.row_len;
+    J.head = S.row_len;
+    J.nvec = 0;
+    if (same) {
+      J.head = std::min<uint64_t>((16 - al) & 15, S.row_len);
+      J.nvec = (S.row_len - J.head) / 16;
+    }
+    uint32_t cm[kMaxSrc * 16];  // coefficients reduced to the field's width, as Plan::matrix does
+    for (size_t q = 0; q < S.nsrcs * S.nrows; ++q) cm[q] = S.coeffs[q] & field_mask(field);
+    build_compact_tables(field, cm, S.nrows, 0, S.nsrcs, 0, G, ht + tn);
+    J.tables = reinterpret_cast<const uint32_t*>(dbase + off_tabs) + tn;
+    tn += S.nsrcs * E * G * kCompactWords;
+    J.gstride = static_cast<uint32_t>(G);
+    J.g0 = 0;
+    J.k = static_cast<uint32_t>(S.nsrcs);
+    J.nrows = static_cast<uint32_t>(S.nrows);
+    J.ovr = S.overwrite ? 1u : 0u;
+    const uint64_t nv_items = (J.nvec + kVecPerItem - 1) / kVecPerItem;
+    const uint64_t tail = J.len - J.head - 16 * J.nvec;
+    const uint64_t ns_items = ((J.head + 3) / 4 + (tail + 3) / 4 + kGroupsPerItem - 1) / kGroupsPerItem;
+    J.nv_items = static_cast<uint32_t>(nv_items);
+    for (uint64_t q = 0; q < nv_items + ns_items; ++q) hi[in++] = make_uint2(static_cast<unsigned>(jn), static_cast<unsigned>(q));
+    ++jn;
+  }
+  if (jn == 0 || in == 0) return 0;
+  std::memset(g_noalloc_host + off_counter, 0, 64);  // the claim counter starts at zero every call
+
+  // ---- one copy, one launch of the work-list kernel on the scratch
+  e = cudaMemcpyAsync(dbase, g_noalloc_host, bytes, cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) {
+    KernelFn fn = kernel_for(E, static_cast<int>(G));
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBatchSmem));
+    if (e == cudaSuccess) {
+      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((in + kClaim - 1) / kClaim, sm_count()));
+      fn<<<grid, kThreads, kBatchSmem, stream>>>(reinterpret_cast<const BatchJob*>(dbase + off_jobs),
+                                                 reinterpret_cast<const uint64_t*>(dbase + off_ptrs),
+                                                 reinterpret_cast<const uint2*>(dbase + off_items),
+                                                 static_cast<uint32_t>(in),
+                                                 reinterpret_cast<uint32_t*>(dbase + off_counter));
+      e = cudaGetLastError();
+    }
+  }
+  if (e != cudaSuccess) {
+    snprintf(msg, msglen, "batch_run_noalloc: CUDA error: %s", cudaGetErrorString(e));
+    return FGFC_ERR_CUDA;
+  }
+  return 0;
 }
 
 }  // namespace fgfc

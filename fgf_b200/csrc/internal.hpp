@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <vector>
 
+#include "../../include/fgf_cuda.h"
 #include "gf_host.hpp"
 
 namespace fgfc {
@@ -82,5 +83,10 @@ void batch_state_destroy(void* state);
 void batch_state_graphs(void* state, bool on);
 void batch_state_stats(const void* state, size_t* launches, size_t* items, int* replayed);
 cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream);
+
+// fgfc_batch_run_noalloc's work (batch.cu): jobs already validated against
+// the ops' rules; returns 0 or an fgfc_status with `msg` set.
+int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStream_t stream, char* msg,
+                size_t msglen);
 
 }  // namespace fgfc

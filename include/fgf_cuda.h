@@ -235,6 +235,49 @@ fgfc_status fgfc_batch_run(fgfc_batch *batch, const fgfc_matrix_job *jobs, size_
 fgfc_status fgfc_batch_stats(const fgfc_batch *batch, size_t *launches, size_t *items,
                              int *graph_replayed);
 
+/* ---------------------------------------------------------------- without allocation */
+
+/* One stripe for fgfc_batch_run_noalloc: like fgfc_matrix_job, but with the
+ * raw coefficient matrix instead of a plan (nsrcs x nrows, term-major: the
+ * order of Plan::matrix(nsrcs, nrows, ..)). */
+typedef struct fgfc_noalloc_job {
+  const uint32_t *coeffs;   /* host, nsrcs * nrows: coeffs[t * nrows + j] multiplies source t into row j */
+  const fgfc_slice *srcs;   /* host array of nsrcs device slices */
+  size_t nsrcs;
+  uint8_t *dst;             /* device destination base */
+  size_t dst_len;
+  const size_t *row_starts; /* host array of nrows offsets into dst, or NULL for rows j * row_len */
+  size_t nrows;
+  size_t row_len;
+  int overwrite;            /* 1 = dot product (overwrite), 0 = accumulate */
+} fgfc_noalloc_job;
+
+/* No counterpart in the reference (a CPU library, which never allocates
+ * device memory at all). The same work as fgfc_batch_run for stripes of one
+ * field, but it allocates nothing: not on the device (no cudaMalloc, no
+ * plan) and not on the host. It is meant for callers that may not allocate
+ * while they run, such as an I/O path that must not take the implicit device
+ * synchronisation and unbounded latency of cudaMalloc, or a process whose
+ * device memory is fully handed to a pool it does not own.
+ *
+ * Its scratch (stripe descriptors, pointers, work items, the claim counter
+ * and every stripe's product tables) lives in one fixed device array of
+ * FGFC_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until
+ * process exit. A submission needing more returns FGFC_ERR_LIMIT; so does a
+ * stripe with more than FGFC_NOALLOC_MAX_ROWS_GF8 rows (Gf8; 8 for Gf16, 4
+ * for Gf32) or more than 64 sources.
+ *
+ * The first call on a device looks up the array's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture. Every call reuses the same array and leaves its contents behind:
+ * calls whose work overlaps on the GPU (different streams, or different
+ * threads without ordering) race on it; calls on one stream are ordered.
+ * Host threads are serialised by a lock around the call itself. */
+#define FGFC_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define FGFC_NOALLOC_MAX_ROWS_GF8 16
+fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job *jobs, size_t njobs,
+                                   fgfc_stream stream);
+
 #ifdef __cplusplus
 }
 #endif
