@@ -63,6 +63,58 @@ class NoAllocJob(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    """`fgfc_server_config`."""
+
+    _fields_ = [
+        ("hbm_budget", c_size),
+        ("staging_bytes", c_size),
+        ("max_batch", c_size),
+        ("max_inflight", c_size),
+        ("plan_cache", c_size),
+        ("max_launch_bytes", c_size),
+        ("plain", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class Request(C.Structure):
+    """`fgfc_request`: one matrix call over host buffers."""
+
+    _fields_ = [
+        ("field", C.c_int),
+        ("coeffs", C.POINTER(c_u32)),
+        ("srcs", C.POINTER(Slice)),
+        ("nsrcs", c_size),
+        ("dst", C.c_void_p),
+        ("dst_len", c_size),
+        ("row_starts", C.POINTER(c_size)),
+        ("nrows", c_size),
+        ("row_len", c_size),
+        ("overwrite", C.c_int),
+    ]
+
+
+class ServerStats(C.Structure):
+    """`fgfc_server_stats`."""
+
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("launches", C.c_uint64),
+        ("plan_hits", C.c_uint64),
+        ("plan_misses", C.c_uint64),
+        ("source_bytes", C.c_uint64),
+        ("peak_device_bytes", C.c_uint64),
+        ("max_batch_seen", C.c_uint64),
+        ("p50_us", C.c_double),
+        ("p99_us", C.c_double),
+        ("mean_us", C.c_double),
+        ("max_us", C.c_double),
+        ("busy_s", C.c_double),
+    ]
+
+
 _SIGS = {
     "fgfc_last_error": (C.c_char_p, []),
     "fgfc_version": (C.c_char_p, []),
@@ -111,6 +163,14 @@ _SIGS = {
     "fgfc_batch_run": (c_status, [C.c_void_p, C.POINTER(MatrixJob), c_size, c_stream]),
     "fgfc_batch_stats": (c_status, [C.c_void_p, C.POINTER(c_size), C.POINTER(c_size), C.POINTER(C.c_int)]),
     "fgfc_batch_run_noalloc": (c_status, [C.c_int, C.POINTER(NoAllocJob), c_size, c_stream]),
+    "fgfc_run_jobs_serial": (c_status, [C.POINTER(MatrixJob), c_size, c_stream]),
+    "fgfc_server_create": (c_status, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "fgfc_server_submit": (c_status, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "fgfc_server_wait": (c_status, [C.c_void_p, C.c_uint64]),
+    "fgfc_server_poll": (c_status, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
+    "fgfc_server_drain": (c_status, [C.c_void_p]),
+    "fgfc_server_get_stats": (c_status, [C.c_void_p, C.POINTER(ServerStats), C.c_int]),
+    "fgfc_server_destroy": (None, [C.c_void_p]),
 }
 
 _lib: C.CDLL | None = None

@@ -83,3 +83,10 @@ class Batch:
         launches, items, rep = C.c_size_t(), C.c_size_t(), C.c_int()
         check(lib().fgfc_batch_stats(self._h, C.byref(launches), C.byref(items), C.byref(rep)))
         return {"launches": launches.value, "items": items.value, "graph_replayed": bool(rep.value)}
+
+
+def run_serial(prepared: Prepared, stream=None) -> None:
+    """Issue each job as its own per-call entry point (dot_product_matrix_with,
+    mul_add_matrix_with or mul_add_matrix_scattered_with) from a native loop:
+    the one-call-per-stripe baseline a batched submission replaces."""
+    check(lib().fgfc_run_jobs_serial(prepared.array, prepared.n, _stream(stream)))

@@ -121,16 +121,18 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
   kc = std::min<size_t>(kc, kMaxSrc);
   if (kc == 0) return fail(FGFC_ERR_LIMIT, "%s: internal tiling failed", name);
 
-  // Alignment class shared by every pointer of the call.
+  // Alignment class shared by every source; the kernels store rows at any
+  // offset (columns are spliced in registers when a row's offset differs).
   uintptr_t al = reinterpret_cast<uintptr_t>(srcs[0]) & 15;
   bool same = true;
   for (size_t t = 0; t < k; ++t) same &= (reinterpret_cast<uintptr_t>(srcs[t]) & 15) == al;
-  for (size_t j = 0; j < m; ++j) same &= (reinterpret_cast<uintptr_t>(rows[j]) & 15) == al;
   same &= (al % E) == 0;
   uint64_t head = len, nvec = 0;
+  bool shift = false;
   if (same) {
     head = std::min<uint64_t>((16 - al) & 15, len);
     nvec = (len - head) / 16;
+    for (size_t j = 0; j < m; ++j) shift |= (reinterpret_cast<uintptr_t>(rows[j]) & 15) != al;
   }
 
   static thread_local MatrixLaunch a;  // large (inline tables): keep off the stack
@@ -143,6 +145,9 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
       a.len = len;
       a.head = head;
       a.nvec = nvec;
+      a.shift = 0;
+      for (size_t j = 0; j < nr; ++j) a.shift |= (reinterpret_cast<uintptr_t>(rows[r0 + j]) & 15) != al;
+      a.shift &= shift ? 1u : 0u;
       a.k = static_cast<uint32_t>(kk);
       a.nrows = static_cast<uint32_t>(nr);
       for (size_t t = 0; t < kk; ++t) a.src[t] = srcs[t0 + t];
@@ -799,6 +804,52 @@ struct fgfc_batch {
   void* state;
 };
 
+namespace fgfc {
+
+// One stripe (all sources of a plan, rows at the given device addresses) as
+// sub-jobs of at most 4 table groups. The vector body is used when every
+// source has the same offset within 16 bytes (a multiple of the element
+// size), whatever the rows' offsets; otherwise the whole stripe takes the
+// 4-byte-group path.
+void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
+                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out) {
+  const int field = plan->field;
+  const int E = field_bytes(field);
+  const int R = 4 / E;
+  const size_t nrows = dsts.size();
+  const uintptr_t al = srcs.empty() ? 0 : (srcs[0] & 15);
+  bool same = (al % E) == 0;
+  for (uint64_t p : srcs) same = same && (p & 15) == al;
+  uint64_t head = row_len, nvec = 0;
+  if (same) {
+    head = std::min<uint64_t>((16 - al) & 15, row_len);
+    nvec = (row_len - head) / 16;
+  }
+  const size_t gtot = (nrows + R - 1) / R;
+  for (size_t g0 = 0; g0 < gtot; g0 += 4) {
+    LoweredJob L;
+    L.field = field;
+    L.tables = plan->dev + plan->off_mat;
+    L.gstride = plan->mat_groups;
+    L.g0 = g0;
+    L.G = std::min<size_t>(4, gtot - g0);
+    L.len = row_len;
+    L.head = head;
+    L.nvec = nvec;
+    L.k = srcs.size();
+    L.nrows = std::min(nrows - g0 * R, L.G * R);
+    L.ovr = overwrite;
+    L.srcs = srcs;
+    L.dsts.assign(dsts.begin() + g0 * R, dsts.begin() + g0 * R + L.nrows);
+    L.shift = false;
+    if (same && nvec)
+      for (uint64_t d : L.dsts) L.shift = L.shift || (d & 15) != al;
+    out.push_back(std::move(L));
+  }
+}
+
+}  // namespace fgfc
+
 extern "C" {
 
 fgfc_status fgfc_batch_create(fgfc_batch** out) {
@@ -877,45 +928,38 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
       }
       continue;
     }
-    const int E = field_bytes(field);
-    const int R = 4 / E;
     std::vector<uint64_t> dsts(J.nrows);
     for (size_t j = 0; j < J.nrows; ++j)
       dsts[j] = reinterpret_cast<uint64_t>(J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len));
     std::vector<uint64_t> srcs(J.nsrcs);
-    const uintptr_t al = reinterpret_cast<uintptr_t>(J.srcs[0].ptr) & 15;
-    bool same = (al % E) == 0;
-    for (size_t t = 0; t < J.nsrcs; ++t) {
-      srcs[t] = reinterpret_cast<uint64_t>(J.srcs[t].ptr);
-      same = same && (srcs[t] & 15) == al;
-    }
-    for (uint64_t d : dsts) same = same && (d & 15) == al;
-    uint64_t head = J.row_len, nvec = 0;
-    if (same) {
-      head = std::min<uint64_t>((16 - al) & 15, J.row_len);
-      nvec = (J.row_len - head) / 16;
-    }
-    const size_t gtot = (J.nrows + R - 1) / R;
-    for (size_t g0 = 0; g0 < gtot; g0 += 4) {
-      LoweredJob L;
-      L.field = field;
-      L.tables = plan->dev + plan->off_mat;
-      L.gstride = plan->mat_groups;
-      L.g0 = g0;
-      L.G = std::min<size_t>(4, gtot - g0);
-      L.len = J.row_len;
-      L.head = head;
-      L.nvec = nvec;
-      L.k = J.nsrcs;
-      L.nrows = std::min(J.nrows - g0 * R, L.G * R);
-      L.ovr = J.overwrite != 0;
-      L.srcs = srcs;
-      L.dsts.assign(dsts.begin() + g0 * R, dsts.begin() + g0 * R + L.nrows);
-      low.push_back(std::move(L));
-    }
+    for (size_t t = 0; t < J.nsrcs; ++t) srcs[t] = reinterpret_cast<uint64_t>(J.srcs[t].ptr);
+    lower_matrix_job(plan, srcs, dsts, J.row_len, J.overwrite != 0, low);
   }
   cudaError_t e = batch_run(batch->state, low, stream);
   return e == cudaSuccess ? ok() : cuda_fail(e, "batch");
+}
+
+fgfc_status fgfc_run_jobs_serial(const fgfc_matrix_job* jobs, size_t njobs, fgfc_stream stream) {
+  if (njobs && !jobs) return fail(FGFC_ERR_ARG, "batch: null argument");
+  for (size_t i = 0; i < njobs; ++i) {
+    const fgfc_matrix_job& J = jobs[i];
+    fgfc_status st;
+    if (J.row_starts) {
+      if (J.overwrite)
+        return fail(FGFC_ERR_ARG, "batch job %zu: scattered rows accumulate; overwrite is not defined", i);
+      st = fgfc_mul_add_matrix_scattered_with(J.dst, J.dst_len, J.row_len, J.row_starts, J.nrows, J.plan, J.srcs,
+                                              J.nsrcs, stream);
+    } else if (J.overwrite) {
+      st = fgfc_dot_product_matrix_with(J.dst, J.dst_len, J.row_len, J.nrows, J.plan, J.srcs, J.nsrcs, stream);
+    } else {
+      st = fgfc_mul_add_matrix_with(J.dst, J.dst_len, J.row_len, J.nrows, J.plan, J.srcs, J.nsrcs, stream);
+    }
+    if (st != FGFC_OK) {
+      t_err = "batch job " + std::to_string(i) + ": " + t_err;
+      return st;
+    }
+  }
+  return ok();
 }
 
 // Same per-job rules as fgfc_batch_run, with the raw coefficient forms'
@@ -961,3 +1005,45 @@ fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job* job
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- shared with serve.cpp
+
+namespace fgfc {
+
+fgfc_status set_error(fgfc_status st, const char* msg) {
+  t_err = msg;
+  return st;
+}
+
+fgfc_status clear_error() { return ok(); }
+
+const char* last_error_text() { return t_err.c_str(); }
+
+// The checks fgfc_batch_run applies to one job, for a job whose buffers are
+// host memory (the serving loop's requests): name is the ops function it
+// stands for.
+fgfc_status validate_matrix_call(int field, const char* name, size_t dst_len, size_t row_len,
+                                 const size_t* row_starts, size_t nrows, const fgfc_slice* srcs, size_t nsrcs,
+                                 const uint32_t* coeffs, int overwrite) {
+  fgfc_status st;
+  if (!valid_field(field)) return fail(FGFC_ERR_ARG, "%s: unknown field", name);
+  if (row_starts) {
+    if (overwrite) return fail(FGFC_ERR_ARG, "%s: scattered rows accumulate; overwrite is not defined", name);
+    if (!check_scattered_rows(field, name, dst_len, row_len, row_starts, nrows, &st)) return st;
+  } else {
+    if (!check_width(field, name, row_len, &st)) return st;
+    size_t used;
+    if (mul_overflows(nrows, row_len, &used)) return fail(FGFC_ERR_OVERFLOW, "%s: row geometry overflows", name);
+    if (dst_len < used)
+      return fail(FGFC_ERR_ROWS, "%s: rows is %zu bytes but %zu rows of %zu bytes need %zu", name, dst_len, nrows,
+                  row_len, used);
+  }
+  if (nsrcs && !srcs) return fail(FGFC_ERR_ARG, "%s: null sources", name);
+  if (nsrcs && nrows && !coeffs) return fail(FGFC_ERR_ARG, "%s: null coefficients", name);
+  for (size_t t = 0; t < nsrcs; ++t)
+    if (srcs[t].len != row_len)
+      return fail(FGFC_ERR_SOURCE, "%s: source %zu is %zu bytes, expected %zu", name, t, srcs[t].len, row_len);
+  return ok();
+}
+
+}  // namespace fgfc

@@ -123,14 +123,21 @@ __device__ __forceinline__ uint32_t out_word(const uint32_t (&acc)[G][NE], int g
 
 // One vector item of a sub-job, for sources [t0, t0 + kk) whose tables are
 // resident; `ovr` overwrites, otherwise the destination is accumulated.
-template <int E, int G>
+// SHIFT: some row is not at the sources' offset within 16 bytes; whole warps
+// then iterate together (the row stores shuffle between lanes) and lanes past
+// the end reload the last column.
+template <int E, int G, bool SHIFT>
 __device__ void vector_item(const BatchJob& J, const uint64_t* ptrs, uint32_t part, uint32_t t0,
                             uint32_t kk, bool ovr) {
   constexpr int NE = 16 / E, R = 4 / E;
-  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane4 = lane * 4u;
   const uint64_t step = static_cast<uint64_t>(J.nv_items) * blockDim.x;
-  for (uint64_t v = static_cast<uint64_t>(part) * blockDim.x + threadIdx.x; v < J.nvec; v += step) {
-    const uint64_t off = J.head + v * 16u;
+  for (uint64_t vb = static_cast<uint64_t>(part) * blockDim.x + threadIdx.x - (SHIFT ? lane : 0u); vb < J.nvec;
+       vb += step) {
+    const uint64_t v = SHIFT ? vb + lane : vb;
+    const bool valid = !SHIFT || v < J.nvec;
+    const uint64_t off = J.head + (valid ? v : J.nvec - 1) * 16u;
     uint32_t acc[G][NE];
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -153,21 +160,17 @@ __device__ void vector_item(const BatchJob& J, const uint64_t* ptrs, uint32_t pa
 #pragma unroll
       for (int rr = 0; rr < R; ++rr) {
         const uint32_t row = g * R + rr;
-        if (row >= J.nrows) continue;
         uint4 o;
         o.x = out_word<E, G, NE>(acc, g, rr, 0);
         o.y = out_word<E, G, NE>(acc, g, rr, 1);
         o.z = out_word<E, G, NE>(acc, g, rr, 2);
         o.w = out_word<E, G, NE>(acc, g, rr, 3);
-        uint4* dp = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off);
-        if (!ovr) {
-          const uint4 d = *dp;
-          o.x ^= d.x;
-          o.y ^= d.y;
-          o.z ^= d.z;
-          o.w ^= d.w;
+        if constexpr (SHIFT) {
+          const bool rv = valid && row < J.nrows;
+          store_vec16(rv ? reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off : nullptr, o, rv, ovr);
+        } else {
+          if (row < J.nrows) put16(reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off, o, ovr);
         }
-        *dp = o;
       }
   }
 }
@@ -224,7 +227,7 @@ __device__ void scalar_item(const BatchJob& J, const uint64_t* ptrs, uint32_t pa
 }
 
 // Persistent work-list kernel for one nibble (E, G) class.
-template <int E, int G>
+template <int E, int G, bool SHIFT>
 __global__ void __launch_bounds__(kThreads, 1)
     batch_kernel(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
                  const uint2* __restrict__ items, uint32_t nitems, uint32_t* counter) {
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         const bool ovr = J.ovr && c == 0;
         if (wi.y < J.nv_items)
-          vector_item<E, G>(J, ptrs, wi.y, t0, kk, ovr);
+          vector_item<E, G, SHIFT>(J, ptrs, wi.y, t0, kk, ovr);
         else
           scalar_item<E, G>(J, ptrs, wi.y - J.nv_items, t0, kk, ovr);
         __syncthreads();  // chunk c's writes precede chunk c + 1's reads of the same rows
@@ -273,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // Work-list kernel for Gf8 sub-jobs of at most 4 rows and exactly K sources.
 // The plan's tables stay resident across consecutive items of one plan.
-template <int K>
+template <int K, bool SHIFT>
 __global__ void __launch_bounds__(kFastThreads, 1)
     batch_fast_kernel(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
                       const uint2* __restrict__ items, uint32_t nitems, uint32_t* counter) {
@@ -311,8 +314,13 @@ __global__ void __launch_bounds__(kFastThreads, 1)
       const bool ovr = J.ovr != 0;
       if (wi.y < J.nv_items) {
         const uint64_t step = static_cast<uint64_t>(J.nv_items) * blockDim.x;
-        for (uint64_t v = static_cast<uint64_t>(wi.y) * blockDim.x + threadIdx.x; v < J.nvec; v += step) {
-          const uint64_t off = J.head + v * 16u;
+        const uint32_t lane = threadIdx.x & 31u;
+        // SHIFT: whole warps iterate together (see vector_item)
+        for (uint64_t vb = static_cast<uint64_t>(wi.y) * blockDim.x + threadIdx.x - (SHIFT ? lane : 0u);
+             vb < J.nvec; vb += step) {
+          const uint64_t v = SHIFT ? vb + lane : vb;
+          const bool valid = !SHIFT || v < J.nvec;
+          const uint64_t off = J.head + (valid ? v : J.nvec - 1) * 16u;
           uint32_t w[K][4];
 #pragma unroll
           for (int t = 0; t < K; ++t) {
@@ -326,7 +334,10 @@ __global__ void __launch_bounds__(kFastThreads, 1)
 #pragma unroll
           for (int e = 0; e < 16; ++e) acc[e] = 0;
           fast_fold<K, 4>(w, acc, r);
-          store_col4(acc, s_dst, J.nrows, off, ovr);
+          if constexpr (SHIFT)
+            store_col4_any(acc, s_dst, J.nrows, off, ovr, valid);
+          else
+            store_col4(acc, s_dst, J.nrows, off, ovr);
         }
       } else {
         const uint64_t tail0 = J.head + J.nvec * 16u;
@@ -384,7 +395,7 @@ struct UniformParams {
 };
 static_assert(sizeof(UniformParams) <= 32000, "launch parameter block too large");
 
-template <int K>
+template <int K, bool SHIFT>
 __global__ void __launch_bounds__(kFastThreads, 1)
     batch_fast_uniform_kernel(const __grid_constant__ UniformParams P) {
   fill_fast<K>(P.tables, nullptr, P.gstride, P.g0);
@@ -392,8 +403,15 @@ __global__ void __launch_bounds__(kFastThreads, 1)
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t vtotal = P.vprefix[P.njobs];
+  const uint32_t lane = threadIdx.x & 31u;
   uint32_t j = 0;
-  for (uint64_t u = tid; u < vtotal; u += stride) {
+  // SHIFT: whole warps iterate together (the row stores shuffle between
+  // lanes; a warp may straddle two stripes) and lanes past the end reload the
+  // last column
+  for (uint64_t ub = tid - (SHIFT ? lane : 0u); ub < vtotal; ub += stride) {
+    const uint64_t u0 = SHIFT ? ub + lane : ub;
+    const bool valid = !SHIFT || u0 < vtotal;
+    const uint64_t u = valid ? u0 : vtotal - 1;
     while (u >= P.vprefix[j + 1]) ++j;
     const UJob& J = P.jobs[j];
     const uint64_t off = J.head + (u - P.vprefix[j]) * 16u;
@@ -410,7 +428,10 @@ __global__ void __launch_bounds__(kFastThreads, 1)
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0;
     fast_fold<K, 4>(w, acc, r);
-    store_col4(acc, J.dst, J.nrows, off, J.ovr != 0);
+    if constexpr (SHIFT)
+      store_col4_any(acc, J.dst, J.nrows, off, J.ovr != 0, valid);
+    else
+      store_col4(acc, J.dst, J.nrows, off, J.ovr != 0);
   }
   const uint64_t gtotal = P.gprefix[P.njobs];
   j = 0;
@@ -446,40 +467,43 @@ __global__ void __launch_bounds__(kFastThreads, 1)
 using KernelFn = void (*)(const BatchJob*, const uint64_t*, const uint2*, uint32_t, uint32_t*);
 using UniformFn = void (*)(UniformParams);
 
-KernelFn kernel_for(int E, int G) {
+template <bool S>
+KernelFn kernel_for_s(int E, int G) {
   switch (E * 8 + G) {
-    case 8 + 1: return batch_kernel<1, 1>;
-    case 8 + 2: return batch_kernel<1, 2>;
-    case 8 + 3: return batch_kernel<1, 3>;
-    case 8 + 4: return batch_kernel<1, 4>;
-    case 16 + 1: return batch_kernel<2, 1>;
-    case 16 + 2: return batch_kernel<2, 2>;
-    case 16 + 3: return batch_kernel<2, 3>;
-    case 16 + 4: return batch_kernel<2, 4>;
-    case 32 + 1: return batch_kernel<4, 1>;
-    case 32 + 2: return batch_kernel<4, 2>;
-    case 32 + 3: return batch_kernel<4, 3>;
-    case 32 + 4: return batch_kernel<4, 4>;
+    case 8 + 1: return batch_kernel<1, 1, S>;
+    case 8 + 2: return batch_kernel<1, 2, S>;
+    case 8 + 3: return batch_kernel<1, 3, S>;
+    case 8 + 4: return batch_kernel<1, 4, S>;
+    case 16 + 1: return batch_kernel<2, 1, S>;
+    case 16 + 2: return batch_kernel<2, 2, S>;
+    case 16 + 3: return batch_kernel<2, 3, S>;
+    case 16 + 4: return batch_kernel<2, 4, S>;
+    case 32 + 1: return batch_kernel<4, 1, S>;
+    case 32 + 2: return batch_kernel<4, 2, S>;
+    case 32 + 3: return batch_kernel<4, 3, S>;
+    case 32 + 4: return batch_kernel<4, 4, S>;
     default: return nullptr;
   }
 }
 
+KernelFn kernel_for(int E, int G, bool shift) { return shift ? kernel_for_s<true>(E, G) : kernel_for_s<false>(E, G); }
+
 #define FGFC_K_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
 
-KernelFn fast_kernel_for(int K) {
+KernelFn fast_kernel_for(int K, bool shift) {
   switch (K) {
 #define FGFC_CASE(k) \
-  case k: return batch_fast_kernel<k>;
+  case k: return shift ? batch_fast_kernel<k, true> : batch_fast_kernel<k, false>;
     FGFC_K_CASES(FGFC_CASE)
 #undef FGFC_CASE
     default: return nullptr;
   }
 }
 
-UniformFn uniform_kernel_for(int K) {
+UniformFn uniform_kernel_for(int K, bool shift) {
   switch (K) {
 #define FGFC_CASE(k) \
-  case k: return batch_fast_uniform_kernel<k>;
+  case k: return shift ? batch_fast_uniform_kernel<k, true> : batch_fast_uniform_kernel<k, false>;
     FGFC_K_CASES(FGFC_CASE)
 #undef FGFC_CASE
     default: return nullptr;
@@ -508,6 +532,7 @@ struct BatchClass {
   std::vector<uint32_t> jobs;  // sub-job indices, plan order
   std::vector<uint2> items;
   bool uniform = false;        // byte-table class whose sub-jobs share one plan
+  bool shift = false;          // its rows are not all at the sources' offset within 16 bytes
 };
 
 struct BatchSlot {
@@ -615,13 +640,14 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) {
     return jobs[a].tables != jobs[c].tables ? jobs[a].tables < jobs[c].tables : jobs[a].g0 < jobs[c].g0;
   });
-  std::map<int, BatchClass> classes;  // key E * 8 + G, or 100 + K for byte-table classes
+  std::map<int, BatchClass> classes;  // key E * 8 + G, or 100 + K for byte-table classes; + 300 if shifted
   for (size_t i : order) {
     const LoweredJob& L = jobs[i];
     const int E = field_bytes(L.field);
     const bool fast = E == 1 && L.G == 1 && L.k >= 1 && L.k <= static_cast<size_t>(kFastMaxK);
-    const int key = fast ? 100 + static_cast<int>(L.k) : E * 8 + static_cast<int>(L.G);
+    const int key = (fast ? 100 + static_cast<int>(L.k) : E * 8 + static_cast<int>(L.G)) + (L.shift ? 300 : 0);
     BatchClass& c = classes[key];
+    c.shift = L.shift;
     c.E = E;
     c.G = static_cast<int>(L.G);
     c.K = fast ? static_cast<int>(L.k) : 0;
@@ -703,7 +729,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   std::string key = std::to_string(reinterpret_cast<uintptr_t>(s.dev)) + ":" + std::to_string(bytes);
   const int sms = sm_count();
   static std::mutex attr_mu;
-  static bool attr_set[256] = {false};
+  static bool attr_set[1024] = {false};
   size_t ci = 0;
   for (auto& kv : classes) {
     const BatchClass& c = kv.second;
@@ -712,9 +738,9 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     Launch L;
     const int akey = kv.first + (c.uniform ? 100 : 0);
     if (c.uniform) {
-      L.ufn = uniform_kernel_for(c.K);
+      L.ufn = uniform_kernel_for(c.K, c.shift);
     } else {
-      L.fn = fast ? fast_kernel_for(c.K) : kernel_for(c.E, c.G);
+      L.fn = fast ? fast_kernel_for(c.K, c.shift) : kernel_for(c.E, c.G, c.shift);
     }
     if (!L.fn && !L.ufn) return cudaErrorInvalidValue;
     L.smem = fast ? fast_smem(c.K) : static_cast<uint32_t>(kBatchSmem);
@@ -971,7 +997,7 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
   // ---- one copy, one launch of the work-list kernel on the scratch
   e = cudaMemcpyAsync(dbase, g_noalloc_host, bytes, cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) {
-    KernelFn fn = kernel_for(E, static_cast<int>(G));
+    KernelFn fn = kernel_for(E, static_cast<int>(G), false);  // rows share the sources' alignment here
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBatchSmem));
     if (e == cudaSuccess) {
       const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((in + kClaim - 1) / kClaim, sm_count()));

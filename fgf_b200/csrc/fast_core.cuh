@@ -147,7 +147,93 @@ __device__ __forceinline__ uint32_t row_word4(const uint32_t* acc, int rr) {
   return prmt(s01, s23, (rr & 1) ? 0x7632u : 0x5410u);
 }
 
-// Store one 16-byte column of up to 4 rows; accumulate unless overwriting.
+// ---------------------------------------------------------------- row stores
+//
+// The vector paths compute 16-byte columns in the alignment of the sources.
+// A destination row may start anywhere (contiguous rows of any length put
+// row j at j * row_len). When a column's destination is dl = addr & 15 bytes
+// past a 16-byte boundary, each lane writes the aligned 16 bytes that end
+// inside its column, spliced from the previous lane's column (one warp
+// shuffle per word) and its own; the ends of a run of contiguous columns are
+// written bytewise. Every byte is written by exactly one lane. All 32 lanes
+// of the warp must call store_vec16 together; lanes without a column pass
+// valid = false.
+
+constexpr unsigned kFullWarp = 0xffffffffu;
+
+// Bytes [s, s + 16) of the 32-byte concatenation P || V, 0 < s < 16.
+__device__ __forceinline__ uint4 splice16(const uint4& P, const uint4& V, uint32_t s) {
+  uint32_t c0, c1, c2, c3, c4;
+  switch (s >> 2) {
+    case 0: c0 = P.x; c1 = P.y; c2 = P.z; c3 = P.w; c4 = V.x; break;
+    case 1: c0 = P.y; c1 = P.z; c2 = P.w; c3 = V.x; c4 = V.y; break;
+    case 2: c0 = P.z; c1 = P.w; c2 = V.x; c3 = V.y; c4 = V.z; break;
+    default: c0 = P.w; c1 = V.x; c2 = V.y; c3 = V.z; c4 = V.w; break;
+  }
+  const uint32_t r = (s & 3u) * 8u;
+  return make_uint4(__funnelshift_r(c0, c1, r), __funnelshift_r(c1, c2, r), __funnelshift_r(c2, c3, r),
+                    __funnelshift_r(c3, c4, r));
+}
+
+// Bytes [b0, b1) of V to p[0 .. b1 - b0), one byte store each.
+__device__ __forceinline__ void put_bytes(uint8_t* p, const uint4& V, uint32_t b0, uint32_t b1, bool ovr) {
+  const uint32_t w[4] = {V.x, V.y, V.z, V.w};
+#pragma unroll
+  for (uint32_t b = 0; b < 16; ++b) {
+    if (b < b0 || b >= b1) continue;
+    const uint8_t v = static_cast<uint8_t>(w[b >> 2] >> (8 * (b & 3u)));
+    uint8_t* q = p + (b - b0);
+    *q = ovr ? v : static_cast<uint8_t>(*q ^ v);
+  }
+}
+
+__device__ __forceinline__ void put16(uint8_t* p, uint4 o, bool ovr) {
+  uint4* dp = reinterpret_cast<uint4*>(p);
+  if (!ovr) {
+    const uint4 d = *dp;
+    o.x ^= d.x;
+    o.y ^= d.y;
+    o.z ^= d.z;
+    o.w ^= d.w;
+  }
+  *dp = o;
+}
+
+// Store the 16-byte column o at p (any alignment); accumulate unless ovr.
+__device__ __forceinline__ void store_vec16(uint8_t* p, const uint4& o, bool valid, bool ovr) {
+  const uint64_t a = reinterpret_cast<uint64_t>(p);
+  const uint32_t dl = static_cast<uint32_t>(a) & 15u;
+  if (__all_sync(kFullWarp, !valid || dl == 0)) {
+    if (valid) put16(p, o, ovr);
+    return;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t ap = __shfl_up_sync(kFullWarp, a, 1);
+  const uint64_t an = __shfl_down_sync(kFullWarp, a, 1);
+  const int vp = __shfl_up_sync(kFullWarp, valid ? 1 : 0, 1);
+  const int vn = __shfl_down_sync(kFullWarp, valid ? 1 : 0, 1);
+  uint4 P;
+  P.x = __shfl_up_sync(kFullWarp, o.x, 1);
+  P.y = __shfl_up_sync(kFullWarp, o.y, 1);
+  P.z = __shfl_up_sync(kFullWarp, o.z, 1);
+  P.w = __shfl_up_sync(kFullWarp, o.w, 1);
+  if (!valid) return;
+  if (dl == 0) {
+    put16(p, o, ovr);
+    return;
+  }
+  const bool prev_ok = lane > 0 && vp && ap + 16 == a;
+  const bool next_ok = lane < 31 && vn && an == a + 16;
+  const uint32_t s = 16u - dl;
+  if (prev_ok)
+    put16(p - dl, splice16(P, o, s), ovr);  // [p - dl, p + s): previous column's tail, then ours
+  else
+    put_bytes(p, o, 0, s, ovr);
+  if (!next_ok) put_bytes(p + s, o, s, 16, ovr);
+}
+
+// Store one 16-byte column of up to 4 rows whose destinations share the
+// sources' alignment; accumulate unless overwriting.
 __device__ __forceinline__ void store_col4(const uint32_t (&acc)[16], uint8_t* const* dst, uint32_t nrows,
                                            uint64_t off, bool ovr) {
 #pragma unroll
@@ -158,15 +244,23 @@ __device__ __forceinline__ void store_col4(const uint32_t (&acc)[16], uint8_t* c
     o.y = row_word4(&acc[4], rr);
     o.z = row_word4(&acc[8], rr);
     o.w = row_word4(&acc[12], rr);
-    uint4* dp = reinterpret_cast<uint4*>(dst[rr] + off);
-    if (!ovr) {
-      const uint4 dv = *dp;
-      o.x ^= dv.x;
-      o.y ^= dv.y;
-      o.z ^= dv.z;
-      o.w ^= dv.w;
-    }
-    *dp = o;
+    put16(dst[rr] + off, o, ovr);
+  }
+}
+
+// The same for rows at any offset. Called by every lane of the warp;
+// `valid` marks lanes holding a column.
+__device__ __forceinline__ void store_col4_any(const uint32_t (&acc)[16], uint8_t* const* dst, uint32_t nrows,
+                                               uint64_t off, bool ovr, bool valid) {
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr) {
+    uint4 o;
+    o.x = row_word4(&acc[0], rr);
+    o.y = row_word4(&acc[4], rr);
+    o.z = row_word4(&acc[8], rr);
+    o.w = row_word4(&acc[12], rr);
+    const bool rv = valid && rr < static_cast<int>(nrows);
+    store_vec16(rv ? dst[rr] + off : nullptr, o, rv, ovr);
   }
 }
 

@@ -38,6 +38,7 @@ struct MatrixLaunch {
   uint32_t nrows;          // rows written by this launch (<= groups * R)
   uint32_t gstride;        // groups per (source, plane) in the compact table array
   uint32_t g0;             // first group of this launch within that array
+  uint32_t shift;          // 1: some row is not at the sources' offset within 16 bytes
   const uint32_t* tables;  // device compact tables, or nullptr for `inline_tab`
   const uint8_t* src[kMaxSrc];
   uint8_t* dst[kMaxRows];
@@ -75,6 +76,7 @@ struct LoweredJob {
   uint64_t len, head, nvec;
   size_t k, nrows;
   bool ovr;
+  bool shift;              // some row is not at the sources' offset within 16 bytes
   std::vector<uint64_t> srcs, dsts;
 };
 
@@ -83,6 +85,18 @@ void batch_state_destroy(void* state);
 void batch_state_graphs(void* state, bool on);
 void batch_state_stats(const void* state, size_t* launches, size_t* items, int* replayed);
 cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream);
+// One stripe of a plan (api.cpp) as sub-jobs for batch_run.
+void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
+                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out);
+
+// Error text of the calling thread (api.cpp), for entry points defined in
+// other files.
+fgfc_status set_error(fgfc_status st, const char* msg);
+fgfc_status clear_error();
+const char* last_error_text();
+fgfc_status validate_matrix_call(int field, const char* name, size_t dst_len, size_t row_len,
+                                 const size_t* row_starts, size_t nrows, const fgfc_slice* srcs, size_t nsrcs,
+                                 const uint32_t* coeffs, int overwrite);
 
 // fgfc_batch_run_noalloc's work (batch.cu): jobs already validated against
 // the ops' rules; returns 0 or an fgfc_status with `msg` set.

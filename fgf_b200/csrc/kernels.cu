@@ -108,18 +108,24 @@ __device__ __forceinline__ uint32_t out_word(const uint32_t (&acc)[G][NE], int g
   }
 }
 
-template <int E, int G, bool OVR>
+// SHIFT: some row is not at the sources' offset within 16 bytes. Then whole
+// warps iterate together (the row stores shuffle between lanes) and lanes
+// past the end reload the last column; otherwise each thread runs alone.
+template <int E, int G, bool OVR, bool SHIFT>
 __global__ void __launch_bounds__(512, (16 / E) * G <= 16 ? 2 : 1)
     matrix_vec_kernel(const __grid_constant__ MatrixLaunch a) {
   constexpr int NE = 16 / E;  // elements per 16-byte step
   constexpr int R = 4 / E;    // rows per group
   fill_tables<E, G>(a);
   __syncthreads();
-  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane4 = lane * 4u;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < a.nvec;
-       v += stride) {
-    const uint64_t off = a.head + v * 16u;
+  for (uint64_t vb = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x - (SHIFT ? lane : 0u);
+       vb < a.nvec; vb += stride) {
+    const uint64_t v = SHIFT ? vb + lane : vb;
+    const bool valid = !SHIFT || v < a.nvec;
+    const uint64_t off = a.head + (valid ? v : a.nvec - 1) * 16u;
     uint32_t acc[G][NE];
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -141,21 +147,17 @@ __global__ void __launch_bounds__(512, (16 / E) * G <= 16 ? 2 : 1)
 #pragma unroll
       for (int rr = 0; rr < R; ++rr) {
         const uint32_t row = g * R + rr;
-        if (row >= a.nrows) continue;
         uint4 o;
         o.x = out_word<E, G, NE>(acc, g, rr, 0);
         o.y = out_word<E, G, NE>(acc, g, rr, 1);
         o.z = out_word<E, G, NE>(acc, g, rr, 2);
         o.w = out_word<E, G, NE>(acc, g, rr, 3);
-        uint4* dp = reinterpret_cast<uint4*>(a.dst[row] + off);
-        if (!OVR) {
-          const uint4 d = *dp;
-          o.x ^= d.x;
-          o.y ^= d.y;
-          o.z ^= d.z;
-          o.w ^= d.w;
+        if constexpr (SHIFT) {
+          const bool rv = valid && row < a.nrows;
+          store_vec16(rv ? a.dst[row] + off : nullptr, o, rv, OVR);
+        } else {
+          if (row < a.nrows) put16(a.dst[row] + off, o, OVR);
         }
-        *dp = o;
       }
   }
 }
@@ -226,13 +228,18 @@ __global__ void __launch_bounds__(256) matrix_scalar_kernel(const __grid_constan
 // kFastMinVec vectors use the nibble kernel, whose tables fill faster.
 constexpr uint64_t kFastMinVec = 1u << 18;  // 4 MiB
 
-template <int K, bool OVR>
+template <int K, bool OVR, bool SHIFT>
 __global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __grid_constant__ MatrixLaunch a) {
   fill_fast<K>(a.tables, a.inline_tab, a.gstride, a.g0);
   const FastRegs r;
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < a.nvec; v += stride) {
-    const uint64_t off = a.head + v * 16u;
+  const uint32_t lane = threadIdx.x & 31u;
+  // SHIFT: whole warps iterate together (see matrix_vec_kernel)
+  for (uint64_t vb = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x - (SHIFT ? lane : 0u);
+       vb < a.nvec; vb += stride) {
+    const uint64_t v = SHIFT ? vb + lane : vb;
+    const bool valid = !SHIFT || v < a.nvec;
+    const uint64_t off = a.head + (valid ? v : a.nvec - 1) * 16u;
     uint32_t w[K][4];
 #pragma unroll
     for (int t = 0; t < K; ++t) {
@@ -246,17 +253,20 @@ __global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __gr
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0;
     fast_fold<K, 4>(w, acc, r);
-    store_col4(acc, a.dst, a.nrows, off, OVR);
+    if constexpr (SHIFT)
+      store_col4_any(acc, a.dst, a.nrows, off, OVR, valid);
+    else
+      store_col4(acc, a.dst, a.nrows, off, OVR);
   }
 }
 
 int g_sms = 0;
 
-template <int K, bool OVR>
+template <int K, bool OVR, bool SHIFT>
 cudaError_t launch_fast_k(const MatrixLaunch& a, cudaStream_t s) {
   static bool configured = false;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR>,
+    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR, SHIFT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          FastLayout<K>::smem);
     if (e != cudaSuccess) return e;
@@ -265,29 +275,34 @@ cudaError_t launch_fast_k(const MatrixLaunch& a, cudaStream_t s) {
   const uint64_t want = (a.nvec + kFastThreads - 1) / kFastThreads;
   const uint64_t cap = static_cast<uint64_t>(sm_count());
   const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
-  matrix_fast_kernel<K, OVR><<<blocks, kFastThreads, FastLayout<K>::smem, s>>>(a);
+  matrix_fast_kernel<K, OVR, SHIFT><<<blocks, kFastThreads, FastLayout<K>::smem, s>>>(a);
   return cudaGetLastError();
+}
+
+template <bool OVR, bool SHIFT>
+cudaError_t launch_fast_s(const MatrixLaunch& a, cudaStream_t s) {
+  switch (a.k) {
+    case 1: return launch_fast_k<1, OVR, SHIFT>(a, s);
+    case 2: return launch_fast_k<2, OVR, SHIFT>(a, s);
+    case 3: return launch_fast_k<3, OVR, SHIFT>(a, s);
+    case 4: return launch_fast_k<4, OVR, SHIFT>(a, s);
+    case 5: return launch_fast_k<5, OVR, SHIFT>(a, s);
+    case 6: return launch_fast_k<6, OVR, SHIFT>(a, s);
+    case 7: return launch_fast_k<7, OVR, SHIFT>(a, s);
+    case 8: return launch_fast_k<8, OVR, SHIFT>(a, s);
+    case 9: return launch_fast_k<9, OVR, SHIFT>(a, s);
+    case 10: return launch_fast_k<10, OVR, SHIFT>(a, s);
+    case 11: return launch_fast_k<11, OVR, SHIFT>(a, s);
+    case 12: return launch_fast_k<12, OVR, SHIFT>(a, s);
+    case 13: return launch_fast_k<13, OVR, SHIFT>(a, s);
+    case 14: return launch_fast_k<14, OVR, SHIFT>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <bool OVR>
 cudaError_t launch_fast(const MatrixLaunch& a, cudaStream_t s) {
-  switch (a.k) {
-    case 1: return launch_fast_k<1, OVR>(a, s);
-    case 2: return launch_fast_k<2, OVR>(a, s);
-    case 3: return launch_fast_k<3, OVR>(a, s);
-    case 4: return launch_fast_k<4, OVR>(a, s);
-    case 5: return launch_fast_k<5, OVR>(a, s);
-    case 6: return launch_fast_k<6, OVR>(a, s);
-    case 7: return launch_fast_k<7, OVR>(a, s);
-    case 8: return launch_fast_k<8, OVR>(a, s);
-    case 9: return launch_fast_k<9, OVR>(a, s);
-    case 10: return launch_fast_k<10, OVR>(a, s);
-    case 11: return launch_fast_k<11, OVR>(a, s);
-    case 12: return launch_fast_k<12, OVR>(a, s);
-    case 13: return launch_fast_k<13, OVR>(a, s);
-    case 14: return launch_fast_k<14, OVR>(a, s);
-    default: return cudaErrorInvalidValue;
-  }
+  return a.shift ? launch_fast_s<OVR, true>(a, s) : launch_fast_s<OVR, false>(a, s);
 }
 
 template <int E, int G, bool OVR>
@@ -295,9 +310,12 @@ cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
   static bool configured = false;
   static int occ_vec = 1;
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR>,
+    cudaError_t e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kMaxSlots * (kSlotBytes + kCompactWords * 4));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kMaxSlots * (kSlotBytes + kCompactWords * 4));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(matrix_scalar_kernel<E, G, OVR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -312,14 +330,14 @@ cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
   } else if (a.nvec) {
     int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, matrix_vec_kernel<E, G, OVR>,
-                                                                  512, smem);
+    auto kern = a.shift ? matrix_vec_kernel<E, G, OVR, true> : matrix_vec_kernel<E, G, OVR, false>;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 512, smem);
     if (e != cudaSuccess) return e;
     occ_vec = occ > 0 ? occ : 1;
     uint64_t want = (a.nvec + 511) / 512;
     uint64_t cap = static_cast<uint64_t>(sms) * occ_vec;
     const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
-    matrix_vec_kernel<E, G, OVR><<<blocks, 512, smem, s>>>(a);
+    kern<<<blocks, 512, smem, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

@@ -234,6 +234,13 @@ fgfc_status fgfc_batch_run(fgfc_batch *batch, const fgfc_matrix_job *jobs, size_
  * whether it replayed a graph. */
 fgfc_status fgfc_batch_stats(const fgfc_batch *batch, size_t *launches, size_t *items,
                              int *graph_replayed);
+/* The same jobs as fgfc_batch_run, each issued as its own call of the
+ * per-call entry point it stands for (dot_product_matrix_with,
+ * mul_add_matrix_with or mul_add_matrix_scattered_with), in order, from a
+ * native loop: the one-call-per-stripe way a caller of the reference's ops
+ * would do it, kept for comparison with the batched launch. Stops at the
+ * first failing job and returns its status. */
+fgfc_status fgfc_run_jobs_serial(const fgfc_matrix_job *jobs, size_t njobs, fgfc_stream stream);
 
 /* ---------------------------------------------------------------- without allocation */
 
@@ -277,6 +284,79 @@ typedef struct fgfc_noalloc_job {
 #define FGFC_NOALLOC_MAX_ROWS_GF8 16
 fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job *jobs, size_t njobs,
                                    fgfc_stream stream);
+
+/* ---------------------------------------------------------------- serving loop */
+
+/* A request loop over HOST buffers. No counterpart in the reference (whose
+ * callers run one `ops` call per stripe on the CPU); each request is exactly
+ * one such call -- dot_product_matrix (overwrite), mul_add_matrix
+ * (accumulate) or mul_add_matrix_scattered (row_starts != NULL) -- with the
+ * same validation and the same bytes in the destination afterwards.
+ *
+ * A worker thread per server admits requests in arrival order while device
+ * memory (hbm_budget) and staging allow, and issues each admitted group as
+ * one launch of the batch work-list kernel; requests that arrive while
+ * earlier launches run are admitted into the next one (continuous batching),
+ * so host-to-device copies, kernels and device-to-host copies of successive
+ * launches overlap on three streams. Coefficient matrices are turned into
+ * device plans once and cached, keyed by a hash of (field, dimensions,
+ * coefficients). Request buffers in page-locked host memory with rows of at
+ * least 256 KiB are copied directly; all others go through the server's
+ * page-locked staging buffers. */
+typedef struct fgfc_server fgfc_server;
+
+typedef struct fgfc_server_config {
+  size_t hbm_budget;    /* device bytes for admitted requests (0: 64 GiB) */
+  size_t staging_bytes; /* page-locked host staging (0: 1 GiB) */
+  size_t max_batch;     /* requests per launch (0: 1024) */
+  size_t max_inflight;  /* launches issued and not yet retired (0: 4) */
+  size_t plan_cache;    /* device plans kept (0: 64); least recently used unreferenced ones go first */
+  size_t max_launch_bytes; /* device bytes per launch (0: 256 MiB), so that a burst is split into
+                              launches whose copies and kernels overlap; a larger request runs alone */
+  int plain;            /* 1: one request at a time through the per-call entry points, synchronously
+                           (the one-call-per-stripe comparison); 0: continuous batching */
+  int device;           /* CUDA device; -1: the device current at creation */
+} fgfc_server_config;
+
+typedef struct fgfc_request {
+  fgfc_field field;
+  const uint32_t *coeffs;   /* nsrcs * nrows, coeffs[t * nrows + j] multiplies source t into row j */
+  const fgfc_slice *srcs;   /* host source shards, row_len bytes each */
+  size_t nsrcs;
+  uint8_t *dst;             /* host destination */
+  size_t dst_len;
+  const size_t *row_starts; /* NULL: rows j * row_len; else scattered rows (accumulate) */
+  size_t nrows;
+  size_t row_len;
+  int overwrite;            /* 1: dot_product_matrix; 0: accumulate */
+} fgfc_request;
+
+typedef struct fgfc_server_stats {
+  uint64_t completed;    /* requests finished (results in host memory) */
+  uint64_t failed;
+  uint64_t launches;     /* kernel submissions (batches, or calls in plain mode) */
+  uint64_t plan_hits, plan_misses;
+  uint64_t source_bytes; /* nsrcs * row_len summed over completed requests */
+  uint64_t peak_device_bytes;
+  uint64_t max_batch_seen;
+  double p50_us, p99_us, mean_us, max_us; /* submit -> result in host memory */
+  double busy_s;         /* first submit -> last completion since the last reset */
+} fgfc_server_stats;
+
+fgfc_status fgfc_server_create(const fgfc_server_config *cfg, fgfc_server **out);
+/* Validates and enqueues; coefficient, source-slice and row_starts arrays are
+ * copied, the host shards and dst must stay valid and untouched until the
+ * request completes. FGFC_ERR_LIMIT if it can never fit the budgets. */
+fgfc_status fgfc_server_submit(fgfc_server *server, const fgfc_request *req, uint64_t *ticket);
+/* Blocks until the request is done and returns its status (its message via
+ * fgfc_last_error); a ticket can be waited for once. */
+fgfc_status fgfc_server_wait(fgfc_server *server, uint64_t ticket);
+/* *done = 1 when the request finished; then behaves as fgfc_server_wait. */
+fgfc_status fgfc_server_poll(fgfc_server *server, uint64_t ticket, int *done);
+/* Blocks until every submitted request has finished. */
+fgfc_status fgfc_server_drain(fgfc_server *server);
+fgfc_status fgfc_server_get_stats(fgfc_server *server, fgfc_server_stats *out, int reset);
+void fgfc_server_destroy(fgfc_server *server);
 
 #ifdef __cplusplus
 }
