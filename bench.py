@@ -321,13 +321,14 @@ def uneven_batch(dev, nstripes: int, reps: int):
     return res
 
 
-def served(dev, nreq: int, seconds_per_load: float):
-    """Serving loop over page-locked host buffers: Poisson arrivals of encode
-    (70%) and reconstruct (30%) requests with mixed geometry, 20 coefficient
-    matrices cached on the device, 64 GiB HBM budget. Saturation throughput
-    first (all requests queued at once), then offered loads of 25-100% of it;
-    each against the same requests served one at a time through the per-call
-    entry points."""
+def served(dev, where: str, nreq: int, seconds_per_load: float):
+    """Serving loop: Poisson arrivals of encode (70%) and reconstruct (30%)
+    requests with mixed geometry, 20 coefficient matrices cached on the
+    device, 64 GiB HBM budget. `where` = "host": shards in page-locked host
+    memory (copied in and out); "device": shards already in HBM (in place).
+    Saturation throughput first (all requests queued at once), then offered
+    loads of 25-100% of it; each against the same requests served one at a
+    time through the per-call entry points."""
     import torch
 
     from fgf_b200 import serve
@@ -345,9 +346,14 @@ def served(dev, nreq: int, seconds_per_load: float):
         dm = decode_rows(field, cm, sv, er)
         mats.append((field, k, len(er), [dm[j][t] for t in range(k) for j in range(len(er))], "reconstruct", er))
     maxL = 4 << 20
-    src_pool = torch.empty(64 * maxL + 4096, dtype=torch.uint8).pin_memory()
-    src_pool.random_(0, 256)
-    ring = torch.empty(3 << 30, dtype=torch.uint8).pin_memory()
+    if where == "host":
+        src_pool = torch.empty(64 * maxL + 4096, dtype=torch.uint8).pin_memory()
+        src_pool.random_(0, 256)
+        ring = torch.empty(3 << 30, dtype=torch.uint8).pin_memory()
+    else:
+        src_pool = torch.empty(64 * maxL + 4096, dtype=torch.uint8, device=dev)
+        src_pool.random_(0, 256)
+        ring = torch.empty(3 << 30, dtype=torch.uint8, device=dev)
     ring_n = ring.numel()
 
     lens = mixed_geometry(nreq, 0xC44)
@@ -359,7 +365,7 @@ def served(dev, nreq: int, seconds_per_load: float):
         L = lens[i][3]
         L -= L % field.BYTES
         L = max(L, field.BYTES)
-        offs = rng.integers(0, 64 * maxL - L, size=k)
+        offs = rng.integers(0, (64 * maxL - L) // 256, size=k) * 256  # shards start 256-byte aligned
         srcs = [src_pool[int(o):int(o) + L] for o in offs]
         if kind == "encode":
             need, starts = m * L, None
@@ -391,7 +397,7 @@ def served(dev, nreq: int, seconds_per_load: float):
             pr.struct.dst = ring_addr + head  # the request is copied at submit; only the host data must wait
             t = srv.submit_prepared(pr)
             live.append((t, head, head + need))
-            head += need
+            head += (need + 255) // 256 * 256
             while live and srv.poll(live[0][0]):
                 live.pop(0)
         srv.drain()
@@ -404,7 +410,8 @@ def served(dev, nreq: int, seconds_per_load: float):
         return {"source_GB/s": round(gbps, 2) if gbps else None, "p50_us": round(st["p50_us"], 1),
                 "p99_us": round(st["p99_us"], 1), "requests": st["completed"], "launches": st["launches"],
                 "max_batch": st["max_batch_seen"], "plan_hits": st["plan_hits"], "plan_misses": st["plan_misses"],
-                "peak_device_GB": round(st["peak_device_bytes"] / 1e9, 2)}
+                "peak_device_GB": round(st["peak_device_bytes"] / 1e9, 2),
+                "queue_us": round(st["queue_us"], 1), "launch_us": round(st["launch_us"], 1)}
 
     srv_b = serve.Server(hbm_budget=64 << 30, staging_bytes=1 << 30)
     srv_p = serve.Server(hbm_budget=1 << 30, staging_bytes=1 << 30, plain=True)  # one request at a time
@@ -429,7 +436,9 @@ def served(dev, nreq: int, seconds_per_load: float):
     return {
         "workload": f"{nreq} requests: 70% encode (dot_product_matrix) / 30% reconstruct "
                     f"(mul_add_matrix_scattered), geometry as the uneven batch, 20 device-cached matrices, "
-                    f"page-locked host shards, HBM budget 64 GiB; mean {mean_src / 1e6:.1f} MB source per request",
+                    + ("page-locked host shards copied in and out" if where == "host" else
+                       "shards already in device memory (served in place)")
+                    + f", HBM budget 64 GiB; mean {mean_src / 1e6:.1f} MB source per request",
         "saturation": {"batched": summary(sat), "plain": summary(sat_plain),
                        "speedup": round((sat["source_bytes"] / sat["busy_s"]) /
                                         (sat_plain["source_bytes"] / sat_plain["busy_s"]), 2)},
@@ -585,9 +594,11 @@ def run_ours(args):
         host_rec = torch.empty(nst, M_PAR, L, dtype=torch.uint8).pin_memory()
         per = max(1, min(nst, 16))
         chunks = [list(range(c, min(nst, c + per))) for c in range(0, nst, per)]
-        bt_e = fb.Batch(graphs=False)
-        enc_c = [bt_e.prepare([enc_jobs[s] for s in ch]) for ch in chunks]
-        rec_c = [bt_e.prepare([rec_jobs[s] for s in ch]) for ch in chunks]
+        # one batch object per chunk: its descriptor slots are reused only by
+        # the same chunk one step later, so issuing never waits on other chunks
+        bt_c = [fb.Batch(graphs=True) for _ in chunks]
+        enc_c = [bt_c[c].prepare([enc_jobs[s] for s in ch]) for c, ch in enumerate(chunks)]
+        rec_c = [bt_c[c].prepare([rec_jobs[s] for s in ch]) for c, ch in enumerate(chunks)]
         s_in = torch.cuda.Stream(dev)
         s_out = torch.cuda.Stream(dev)
         ev_in = [torch.cuda.Event() for _ in chunks]
@@ -606,8 +617,8 @@ def run_ours(args):
                 ev_in[c].record(s_in)
                 stream.wait_event(ev_in[c])
                 stream.wait_event(ev_out[c])    # the previous step's results have left
-                bt_e.run_prepared(enc_c[c], stream)
-                bt_e.run_prepared(rec_c[c], stream)
+                bt_c[c].run_prepared(enc_c[c], stream)
+                bt_c[c].run_prepared(rec_c[c], stream)
                 ev_run[c].record(stream)
                 s_out.wait_event(ev_run[c])
                 with torch.cuda.stream(s_out):
@@ -617,7 +628,8 @@ def run_ours(args):
                             host_rec[s, j].copy_(row(s, e), non_blocking=True)
                 ev_out[c].record(s_out)
 
-        e2e_step()
+        for _ in range(3):  # warm-up: every descriptor slot captures its graph
+            e2e_step()
         torch.cuda.synchronize()
         want_par = host_par.clone()
         es = max(1, min(args.steps, 5))
@@ -651,7 +663,10 @@ def run_ours(args):
         extra["uneven_batch"] = uneven_batch(dev, args.uneven_stripes, 5)
         torch.cuda.empty_cache()  # its buffers are free now; hand them back before the serving loop allocates
     if world == 1 and not args.no_serve:
-        extra["served"] = served(dev, args.serve_requests, 0.5)
+        extra["served"] = {"host": served(dev, "host", args.serve_requests, 0.5)}
+        torch.cuda.empty_cache()
+        extra["served"]["device"] = served(dev, "device", 4 * args.serve_requests, 0.25)
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:

@@ -112,6 +112,8 @@ class ServerStats(C.Structure):
         ("mean_us", C.c_double),
         ("max_us", C.c_double),
         ("busy_s", C.c_double),
+        ("queue_us", C.c_double),
+        ("launch_us", C.c_double),
     ]
 
 

@@ -321,6 +321,10 @@ __global__ void __launch_bounds__(kFastThreads, 1)
           const uint64_t v = SHIFT ? vb + lane : vb;
           const bool valid = !SHIFT || v < J.nvec;
           const uint64_t off = J.head + (valid ? v : J.nvec - 1) * 16u;
+          if (v + step < J.nvec) {  // this thread's next column: into L2 now
+#pragma unroll
+            for (int t = 0; t < K; ++t) prefetch_l2(s_src[t] + off + step * 16u);
+          }
           uint32_t w[K][4];
 #pragma unroll
           for (int t = 0; t < K; ++t) {
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(kFastThreads, 1)
   const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const uint64_t vtotal = P.vprefix[P.njobs];
   const uint32_t lane = threadIdx.x & 31u;
-  uint32_t j = 0;
+  uint32_t j = 0, jn = 0;
   // SHIFT: whole warps iterate together (the row stores shuffle between
   // lanes; a warp may straddle two stripes) and lanes past the end reload the
   // last column
@@ -415,6 +419,14 @@ __global__ void __launch_bounds__(kFastThreads, 1)
     while (u >= P.vprefix[j + 1]) ++j;
     const UJob& J = P.jobs[j];
     const uint64_t off = J.head + (u - P.vprefix[j]) * 16u;
+    const uint64_t un = u + stride;  // this thread's next column: into L2 now
+    if (un < vtotal) {
+      while (un >= P.vprefix[jn + 1]) ++jn;
+      const UJob& JN = P.jobs[jn];
+      const uint64_t offn = JN.head + (un - P.vprefix[jn]) * 16u;
+#pragma unroll
+      for (int t = 0; t < K; ++t) prefetch_l2(JN.src[t] + offn);
+    }
     uint32_t w[K][4];
 #pragma unroll
     for (int t = 0; t < K; ++t) {
@@ -535,6 +547,12 @@ struct BatchClass {
   bool shift = false;          // its rows are not all at the sources' offset within 16 bytes
 };
 
+// Descriptor slots used round robin: a submission waits (on the host) only
+// for the one kBatchSlots submissions before it, so that many can be queued
+// on the GPU at once. With an even count, alternating submissions keep their
+// own slots and replay their graphs.
+constexpr int kBatchSlots = 4;
+
 struct BatchSlot {
   uint8_t* host = nullptr;  // pinned
   uint8_t* dev = nullptr;
@@ -544,12 +562,18 @@ struct BatchSlot {
   std::string key;
 };
 
+// Classes of one submission run on side streams forked from the caller's
+// stream, so that small classes share the GPU instead of queueing.
+constexpr int kSideStreams = 4;
+
 struct BatchState {
   std::vector<UniformParams> uparams;
-  BatchSlot slot[2];
+  BatchSlot slot[kBatchSlots];
   int next = 0;
   bool graphs = true;
   cudaStream_t capture = nullptr;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t fork = nullptr, join[kSideStreams] = {};
   size_t last_launches = 0, last_items = 0;
   int last_replayed = 0;
   std::mutex mu;
@@ -593,6 +617,11 @@ void batch_state_destroy(void* p) {
     if (s.done) cudaEventDestroy(s.done);
   }
   if (b->capture) cudaStreamDestroy(b->capture);
+  for (int i = 0; i < kSideStreams; ++i) {
+    if (b->side[i]) cudaStreamDestroy(b->side[i]);
+    if (b->join[i]) cudaEventDestroy(b->join[i]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
   delete b;
 }
 
@@ -659,7 +688,15 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     for (uint32_t i : c.jobs)
       c.uniform = c.uniform && jobs[i].tables == jobs[c.jobs[0]].tables && jobs[i].g0 == jobs[c.jobs[0]].g0;
     if (c.uniform) continue;
-    const uint64_t per_vec = c.K ? kFastVecPerItem : kVecPerItem;
+    // Columns per item: up to 8 per thread, fewer when the class is too
+    // small to give every SM a few items (a small class runs beside the
+    // others on its own stream, see enqueue).
+    const uint64_t threads = c.K ? kFastThreads : kThreads;
+    uint64_t total = 0;
+    for (uint32_t i : c.jobs) total += jobs[i].nvec;
+    const uint64_t want = (total + 4 * static_cast<uint64_t>(sm_count()) - 1) / (4 * static_cast<uint64_t>(sm_count()));
+    const uint64_t per_vec = std::min<uint64_t>(c.K ? kFastVecPerItem : kVecPerItem,
+                                                std::max<uint64_t>(threads, (want + threads - 1) / threads * threads));
     const uint64_t per_grp = c.K ? kFastGroupsPerItem : kGroupsPerItem;
     for (uint32_t i : c.jobs) {
       const LoweredJob& L = jobs[i];
@@ -692,7 +729,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   const size_t bytes = off;
 
   BatchSlot& s = b->slot[b->next];
-  b->next ^= 1;
+  b->next = (b->next + 1) % kBatchSlots;
   cudaError_t e = cudaSuccess;
   if (s.done) {
     e = cudaEventSynchronize(s.done);  // the previous submission out of this slot finished
@@ -805,18 +842,43 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   const BatchJob* djobs = reinterpret_cast<const BatchJob*>(s.dev + off_jobs);
   const uint64_t* dptrs = reinterpret_cast<const uint64_t*>(s.dev + off_ptrs);
 
+  const int nside = launches.size() > 1 ? static_cast<int>(std::min<size_t>(launches.size(), kSideStreams)) : 0;
+  for (int i = 0; i < nside; ++i) {
+    if (!b->side[i]) {
+      e = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nside && !b->fork) {
+    e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  // blob copy on the caller's stream; with several classes, fork to the side
+  // streams (class i on stream i % kSideStreams) and join back
   auto enqueue = [&](cudaStream_t st) -> cudaError_t {
     cudaError_t err = cudaMemcpyAsync(s.dev, s.host, bytes, cudaMemcpyHostToDevice, st);
     if (err != cudaSuccess) return err;
-    for (const Launch& L : launches) {
+    if (nside) {
+      err = cudaEventRecord(b->fork, st);
+      for (int i = 0; i < nside && err == cudaSuccess; ++i) err = cudaStreamWaitEvent(b->side[i], b->fork, 0);
+      if (err != cudaSuccess) return err;
+    }
+    for (size_t li = 0; li < launches.size(); ++li) {
+      const Launch& L = launches[li];
+      cudaStream_t ls = nside ? b->side[li % nside] : st;
       if (L.ufn)
-        L.ufn<<<L.grid, L.threads, L.smem, st>>>(uparams[L.uparam]);
+        L.ufn<<<L.grid, L.threads, L.smem, ls>>>(uparams[L.uparam]);
       else
-        L.fn<<<L.grid, L.threads, L.smem, st>>>(djobs, dptrs, L.items, L.n, L.counter);
+        L.fn<<<L.grid, L.threads, L.smem, ls>>>(djobs, dptrs, L.items, L.n, L.counter);
       err = cudaGetLastError();
       if (err != cudaSuccess) return err;
     }
-    return cudaSuccess;
+    for (int i = 0; i < nside && err == cudaSuccess; ++i) {
+      err = cudaEventRecord(b->join[i], b->side[i]);
+      if (err == cudaSuccess) err = cudaStreamWaitEvent(st, b->join[i], 0);
+    }
+    return err;
   };
 
   b->last_launches = launches.size();

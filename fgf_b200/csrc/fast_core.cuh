@@ -28,6 +28,11 @@ __device__ __forceinline__ uint4 ldg16(const uint8_t* p) {
   return v;
 }
 
+// Pull a line into L2 ahead of its load (the next grid-stride iteration's
+// column); this keeps more DRAM requests in flight than the registers of
+// 1024-thread CTAs allow.
+__device__ __forceinline__ void prefetch_l2(const uint8_t* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ---------------------------------------------------------------- byte-table layout
 //
 // Gf8 fields with at most 4 rows (one table group) and a compile-time number

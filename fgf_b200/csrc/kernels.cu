@@ -240,6 +240,10 @@ __global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __gr
     const uint64_t v = SHIFT ? vb + lane : vb;
     const bool valid = !SHIFT || v < a.nvec;
     const uint64_t off = a.head + (valid ? v : a.nvec - 1) * 16u;
+    if (v + stride < a.nvec) {  // this thread's next column: into L2 now
+#pragma unroll
+      for (int t = 0; t < K; ++t) prefetch_l2(a.src[t] + off + stride * 16u);
+    }
     uint32_t w[K][4];
 #pragma unroll
     for (int t = 0; t < K; ++t) {

@@ -9,12 +9,14 @@
 //              host-to-device copy (direct requests row by row), run every
 //              admitted request as one submission of the batch work-list
 //              kernel, and queue the device-to-host copy of all results;
-//   retire  -- when a launch's last copy has landed (signalled by a host
-//              function on the copy-out stream), move staged results into the
-//              callers' buffers, free the blocks and complete the requests.
+//   retire  -- when a launch's last copy has landed (its event on the
+//              copy-out stream, polled by the worker), move staged results
+//              into the callers' buffers, free the blocks and complete the
+//              requests.
 // The loop admits new requests while earlier launches are still on the GPU,
-// so their copies and kernels overlap (continuous batching). Plain mode runs
-// one request at a time through the per-call entry points instead, for
+// so their copies and kernels overlap (continuous batching). Requests whose
+// buffers are all device memory skip the copies and run in place. Plain mode
+// runs one request at a time through the per-call entry points instead, for
 // comparison.
 #include <cuda_runtime.h>
 
@@ -121,6 +123,9 @@ struct Req {
   size_t k = 0, m = 0, L = 0, Ls = 0;  // sources, rows, row length, device row stride
   bool ovr = false;
   bool direct = false;                 // page-locked buffers with long rows: no staging
+  bool on_device = false;              // every buffer is device memory: used in place, no copies
+  bool scattered = false;              // row_starts given (mul_add_matrix_scattered)
+  size_t dst_len = 0;
   std::vector<uint32_t> coeffs;        // term-major, masked to the field
   std::vector<const uint8_t*> src;
   std::vector<size_t> starts;          // host row offsets into dst
@@ -128,13 +133,13 @@ struct Req {
   uint64_t key = 0;
   PlanEntry* plan = nullptr;
   size_t d_src = 0, d_rows = 0;        // offsets inside the launch's device block
-  Clock::time_point t0;
+  Clock::time_point t0, t_issue;
   fgfc_status status = FGFC_OK;
   std::string err;
   bool done = false;
 
-  size_t dev_bytes() const { return (k + m) * Ls; }
-  size_t stg_bytes() const { return direct ? 0 : k * Ls + (ovr ? m * Ls : 2 * m * Ls); }
+  size_t dev_bytes() const { return on_device ? 0 : (k + m) * Ls; }
+  size_t stg_bytes() const { return direct || on_device ? 0 : k * Ls + (ovr ? m * Ls : 2 * m * Ls); }
 };
 
 struct Launch {
@@ -143,19 +148,27 @@ struct Launch {
   size_t stg_off = 0, stg_len = 0;  // staging arena block
   size_t in_len = 0;                // staged input image: device [0, in_len) of the block
   size_t out0 = 0, out_len = 0;     // staged results: device [out0, out0 + out_len), staging [in_len, ...)
-  cudaEvent_t ev_in = nullptr, ev_done = nullptr;
-  std::atomic<bool> landed{false};
-  fgfc_server* srv = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_done = nullptr, ev_out = nullptr;  // ev_out: the last copy has landed
+  bool failed = false;               // issuing stopped early; everything queued has been waited for
+  Clock::time_point t_issue;
   cudaError_t err = cudaSuccess;
 };
 
-bool host_locked(const void* p) {
+// cudaMemoryTypeHost (page-locked), cudaMemoryTypeDevice (with its device)
+// or cudaMemoryTypeUnregistered (pageable).
+cudaMemoryType where(const void* p, int* device) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return cudaMemoryTypeUnregistered;
   }
-  return a.type == cudaMemoryTypeHost;
+  *device = a.device;
+  return a.type;
+}
+
+bool host_locked(const void* p) {
+  int d = 0;
+  return where(p, &d) == cudaMemoryTypeHost;
 }
 
 }  // namespace
@@ -187,6 +200,8 @@ struct fgfc_server {
 
   // statistics (under mu)
   std::vector<double> lat_us;
+  double queue_sum = 0, launch_sum = 0;
+  uint64_t launch_n = 0;
   uint64_t completed = 0, failed = 0, launches = 0, hits = 0, misses = 0, src_bytes = 0, peak_dev = 0,
            max_batch_seen = 0;
   Clock::time_point first_submit, last_done;
@@ -200,21 +215,6 @@ struct fgfc_server {
   void retire(Launch* L);
   void finish(Req* r, fgfc_status st, const std::string& err);
 };
-
-namespace {
-
-// Runs on a CUDA driver thread once a launch's last copy has landed. It may
-// make no CUDA calls. The flag is set under the server's lock, which the
-// worker holds when it reads it, so the server outlives this function.
-void CUDART_CB on_landed(void* p) {
-  Launch* L = static_cast<Launch*>(p);
-  fgfc_server* s = L->srv;
-  std::lock_guard<std::mutex> lk(s->mu);
-  L->landed.store(true, std::memory_order_release);
-  s->cv.notify_all();
-}
-
-}  // namespace
 
 bool fgfc_server::acquire_plan(Req* r) {
   auto range = plan_index.equal_range(r->key);
@@ -281,6 +281,7 @@ void fgfc_server::finish(Req* r, fgfc_status st, const std::string& err) {
     completed++;
     src_bytes += r->k * r->L;
     lat_us.push_back(std::chrono::duration<double, std::micro>(now - r->t0).count());
+    if (r->t_issue > r->t0) queue_sum += std::chrono::duration<double, std::micro>(r->t_issue - r->t0).count();
   } else {
     failed++;
   }
@@ -293,20 +294,21 @@ void fgfc_server::finish(Req* r, fgfc_status st, const std::string& err) {
 // stages inputs, and queues copy-in, kernel and copy-out.
 void fgfc_server::issue(Launch* L) {
   // device layout: [staged sources | staged accumulate rows | staged overwrite rows | direct requests]
+  auto staged = [](const Req* r) { return !r->direct && !r->on_device; };
   size_t off = 0;
   for (Req* r : L->reqs)
-    if (!r->direct) {
+    if (staged(r)) {
       r->d_src = off;
       off += r->k * r->Ls;
     }
   const size_t acc0 = off;
   for (Req* r : L->reqs)
-    if (!r->direct && !r->ovr) {
+    if (staged(r) && !r->ovr) {
       r->d_rows = off;
       off += r->m * r->Ls;
     }
   for (Req* r : L->reqs)
-    if (!r->direct && r->ovr) {
+    if (staged(r) && r->ovr) {
       r->d_rows = off;
       off += r->m * r->Ls;
     }
@@ -322,7 +324,7 @@ void fgfc_server::issue(Launch* L) {
   // accumulate rows are inputs too: the staged input image is device [0, first overwrite row)
   size_t in_end = acc0;
   for (Req* r : L->reqs)
-    if (!r->direct && !r->ovr) in_end = std::max(in_end, r->d_rows + r->m * r->Ls);
+    if (staged(r) && !r->ovr) in_end = std::max(in_end, r->d_rows + r->m * r->Ls);
   L->in_len = in_end;
   L->out0 = acc0;
   L->out_len = out_end - acc0;
@@ -333,7 +335,7 @@ void fgfc_server::issue(Launch* L) {
   cudaError_t e = cudaSuccess;
   // stage inputs (CPU copies into page-locked memory), then one copy in
   for (Req* r : L->reqs) {
-    if (r->direct) continue;
+    if (!staged(r)) continue;
     for (size_t t = 0; t < r->k; ++t) std::memcpy(sbase + r->d_src + t * r->Ls, r->src[t], r->L);
     if (!r->ovr)
       for (size_t j = 0; j < r->m; ++j) std::memcpy(sbase + r->d_rows + j * r->Ls, r->dst + r->starts[j], r->L);
@@ -358,8 +360,10 @@ void fgfc_server::issue(Launch* L) {
     for (Req* r : L->reqs) {
       sp.resize(r->k);
       dp.resize(r->m);
-      for (size_t t = 0; t < r->k; ++t) sp[t] = reinterpret_cast<uint64_t>(dbase + r->d_src + t * r->Ls);
-      for (size_t j = 0; j < r->m; ++j) dp[j] = reinterpret_cast<uint64_t>(dbase + r->d_rows + j * r->Ls);
+      for (size_t t = 0; t < r->k; ++t)
+        sp[t] = reinterpret_cast<uint64_t>(r->on_device ? r->src[t] : dbase + r->d_src + t * r->Ls);
+      for (size_t j = 0; j < r->m; ++j)
+        dp[j] = reinterpret_cast<uint64_t>(r->on_device ? r->dst + r->starts[j] : dbase + r->d_rows + j * r->Ls);
       lower_matrix_job(r->plan->plan, sp, dp, r->L, r->ovr, low);
     }
     e = batch_run(batch, low, s_run);
@@ -375,14 +379,14 @@ void fgfc_server::issue(Launch* L) {
     for (size_t j = 0; j < r->m && e == cudaSuccess; ++j)
       e = cudaMemcpyAsync(r->dst + r->starts[j], dbase + r->d_rows + j * r->Ls, r->L, cudaMemcpyDeviceToHost, s_out);
   }
-  if (e == cudaSuccess) e = cudaLaunchHostFunc(s_out, on_landed, L);
+  if (e == cudaSuccess) e = cudaEventRecord(L->ev_out, s_out);
   if (e != cudaSuccess) {
     // nothing further was queued for this launch; wait for what was, then fail it
     cudaStreamSynchronize(s_in);
     cudaStreamSynchronize(s_run);
     cudaStreamSynchronize(s_out);
     L->err = e;
-    L->landed.store(true, std::memory_order_release);
+    L->failed = true;
   }
 }
 
@@ -390,12 +394,14 @@ void fgfc_server::retire(Launch* L) {
   const uint8_t* sout = stg + L->stg_off + L->in_len;
   if (L->err == cudaSuccess) {
     for (Req* r : L->reqs) {
-      if (r->direct) continue;
+      if (r->direct || r->on_device) continue;
       for (size_t j = 0; j < r->m; ++j) std::memcpy(r->dst + r->starts[j], sout + (r->d_rows - L->out0) + j * r->Ls, r->L);
     }
   }
   for (Req* r : L->reqs) release_plan(r);
   std::lock_guard<std::mutex> lk(mu);
+  launch_sum += std::chrono::duration<double, std::micro>(Clock::now() - L->t_issue).count();
+  launch_n++;
   dev_arena.release(L->dev_off, L->dev_len);
   stg_arena.release(L->stg_off, L->stg_len);
   const std::string msg =
@@ -403,6 +409,7 @@ void fgfc_server::retire(Launch* L) {
   for (Req* r : L->reqs) finish(r, L->err == cudaSuccess ? FGFC_OK : FGFC_ERR_CUDA, msg);
   cudaEventDestroy(L->ev_in);
   cudaEventDestroy(L->ev_done);
+  cudaEventDestroy(L->ev_out);
 }
 
 // Plain mode: one request, one call of the per-call entry point, synchronously.
@@ -410,6 +417,30 @@ void fgfc_server::run_plain(Req* r) {
   cudaError_t e = cudaSuccess;
   fgfc_status st = FGFC_OK;
   std::string err;
+  if (r->on_device) {
+    // in place: exactly the call the request stands for
+    std::vector<fgfc_slice> sl(r->k);
+    for (size_t t = 0; t < r->k; ++t) sl[t] = fgfc_slice{r->src[t], r->L};
+    if (r->scattered)
+      st = fgfc_mul_add_matrix_scattered_with(r->dst, r->dst_len, r->L, r->starts.data(), r->m, r->plan->plan,
+                                              sl.data(), r->k, s_run);
+    else if (r->ovr)
+      st = fgfc_dot_product_matrix_with(r->dst, r->dst_len, r->L, r->m, r->plan->plan, sl.data(), r->k, s_run);
+    else
+      st = fgfc_mul_add_matrix_with(r->dst, r->dst_len, r->L, r->m, r->plan->plan, sl.data(), r->k, s_run);
+    if (st != FGFC_OK) err = last_error_text();
+    e = cudaStreamSynchronize(s_run);
+    if (e != cudaSuccess) {
+      st = FGFC_ERR_CUDA;
+      err = std::string("server: CUDA error: ") + cudaGetErrorString(e);
+    }
+    release_plan(r);
+    std::lock_guard<std::mutex> lk(mu);
+    launches++;
+    max_batch_seen = std::max<uint64_t>(max_batch_seen, 1);
+    finish(r, st, err);
+    return;
+  }
   uint8_t* d = dev;  // the whole arena serves one request at a time
   uint8_t* s = stg;
   const size_t src_bytes_ = r->k * r->Ls;
@@ -476,10 +507,17 @@ void fgfc_server::run_plain(Req* r) {
 void fgfc_server::run() {
   cudaSetDevice(device);
   std::unique_lock<std::mutex> lk(mu);
+  Clock::time_point idle_since = Clock::now();
   for (;;) {
     bool progressed = false;
-    // retire landed launches, oldest first
-    while (!inflight.empty() && inflight.front()->landed.load(std::memory_order_acquire)) {
+    // retire launches whose last copy has landed, oldest first
+    while (!inflight.empty()) {
+      Launch* F = inflight.front().get();
+      if (!F->failed) {
+        const cudaError_t q = cudaEventQuery(F->ev_out);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) F->err = q;
+      }
       std::unique_ptr<Launch> L = std::move(inflight.front());
       inflight.pop_front();
       lk.unlock();
@@ -491,6 +529,7 @@ void fgfc_server::run() {
       if (!pending.empty()) {
         Req* r = pending.front();
         pending.pop_front();
+        r->t_issue = Clock::now();
         lk.unlock();
         if (acquire_plan(r)) {
           run_plain(r);
@@ -504,7 +543,6 @@ void fgfc_server::run() {
     } else if (!pending.empty() && inflight.size() < cfg.max_inflight) {
       // admit in arrival order while the blocks still fit
       auto L = std::make_unique<Launch>();
-      L->srv = this;
       size_t dbytes = 0, sbytes = 0;
       while (!pending.empty() && L->reqs.size() < cfg.max_batch) {
         Req* r = pending.front();
@@ -532,6 +570,8 @@ void fgfc_server::run() {
         max_batch_seen = std::max<uint64_t>(max_batch_seen, L->reqs.size());
         launches++;
         Launch* raw = L.get();
+        raw->t_issue = Clock::now();
+        for (Req* r : raw->reqs) r->t_issue = raw->t_issue;
         inflight.push_back(std::move(L));
         lk.unlock();
         // plans (a miss uploads tables), events, then the launch itself
@@ -547,9 +587,10 @@ void fgfc_server::run() {
         }
         cudaError_t e = cudaEventCreateWithFlags(&raw->ev_in, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&raw->ev_done, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&raw->ev_out, cudaEventDisableTiming);
         if (e != cudaSuccess) {
           raw->err = e;
-          raw->landed.store(true, std::memory_order_release);
+          raw->failed = true;
         } else {
           issue(raw);
         }
@@ -557,10 +598,20 @@ void fgfc_server::run() {
         progressed = true;
       }
     }
-    if (progressed) continue;
+    if (progressed) {
+      idle_since = Clock::now();
+      continue;
+    }
     if (stop && pending.empty() && inflight.empty()) break;
-    // sleep until a submission or a landed launch; the timeout is a backstop
-    cv.wait_for(lk, std::chrono::milliseconds(2));
+    if (inflight.empty()) {
+      cv.wait(lk, [&] { return stop || !pending.empty(); });  // nothing on the GPU: sleep until a submission
+    } else if (Clock::now() - idle_since < std::chrono::microseconds(500)) {
+      lk.unlock();  // launches in flight: poll their events, briefly yielding
+      std::this_thread::yield();
+      lk.lock();
+    } else {
+      cv.wait_for(lk, std::chrono::microseconds(50));  // long kernels: poll less often
+    }
   }
 }
 
@@ -637,8 +688,23 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
   h = fnv1a(h, &r->m, sizeof r->m);
   h = fnv1a(h, r->coeffs.data(), r->coeffs.size() * 4);
   r->key = h;
+  r->scattered = q->row_starts != nullptr;
+  r->dst_len = q->dst_len;
   const bool trivial = r->m == 0 || r->L == 0 || r->k == 0;
-  if (!trivial && r->L >= kDirectMin) {
+  if (!trivial) {
+    // all device memory of this server's device (used in place), or all host memory
+    int dev = -1, ndev = 0, nbuf = 0;
+    auto on_dev = [&](const void* p) {
+      ++nbuf;
+      if (where(p, &dev) == cudaMemoryTypeDevice && dev == s->device) ++ndev;
+    };
+    on_dev(r->dst);
+    for (size_t t = 0; t < r->k; ++t) on_dev(r->src[t]);
+    if (ndev && ndev != nbuf)
+      return set_error(FGFC_ERR_ARG, "server: a request's buffers must all be host memory or all device memory");
+    r->on_device = ndev == nbuf;
+  }
+  if (!trivial && !r->on_device && r->L >= kDirectMin) {
     bool locked = host_locked(r->dst) && host_locked(r->dst + q->dst_len - 1);
     for (size_t t = 0; t < r->k && locked; ++t) locked = host_locked(r->src[t]) && host_locked(r->src[t] + r->L - 1);
     r->direct = locked;
@@ -657,8 +723,16 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
   s->outstanding++;
   if (trivial) {
     // no sources: an overwrite clears the rows; everything else is a no-op
-    if (raw->ovr && raw->L)
-      for (size_t j = 0; j < raw->m; ++j) std::memset(raw->dst + raw->starts[j], 0, raw->L);
+    if (raw->ovr && raw->L && raw->m) {
+      int dev = -1;
+      if (where(raw->dst, &dev) == cudaMemoryTypeDevice) {
+        // device rows: cleared in stream order on the request stream
+        for (size_t j = 0; j < raw->m; ++j) cudaMemsetAsync(raw->dst + raw->starts[j], 0, raw->L, s->s_run);
+        cudaStreamSynchronize(s->s_run);
+      } else {
+        for (size_t j = 0; j < raw->m; ++j) std::memset(raw->dst + raw->starts[j], 0, raw->L);
+      }
+    }
     s->finish(raw, FGFC_OK, std::string());
     return clear_error();
   }
@@ -730,8 +804,12 @@ fgfc_status fgfc_server_get_stats(fgfc_server* s, fgfc_server_stats* out, int re
   }
   if (s->have_first && s->completed + s->failed)
     out->busy_s = std::chrono::duration<double>(s->last_done - s->first_submit).count();
+  if (s->completed) out->queue_us = s->queue_sum / static_cast<double>(s->completed);
+  if (s->launch_n) out->launch_us = s->launch_sum / static_cast<double>(s->launch_n);
   if (reset) {
     s->lat_us.clear();
+    s->queue_sum = s->launch_sum = 0;
+    s->launch_n = 0;
     s->completed = s->failed = s->launches = s->hits = s->misses = s->src_bytes = s->peak_dev =
         s->max_batch_seen = 0;
     s->have_first = false;

@@ -1,10 +1,11 @@
-"""Serving loop over host buffers (`fgfc_server_*`).
+"""Serving loop (`fgfc_server_*`).
 
 No reference counterpart: fgf's callers issue one `ops` call per stripe on
 the CPU. Each request here is exactly one such call -- `dot_product_matrix`
 (overwrite), `mul_add_matrix` (accumulate) or `mul_add_matrix_scattered`
-(src/ops.rs:675-941) -- over host memory, validated the same way and leaving
-the same bytes in the destination. The native worker admits requests in
+(src/ops.rs:675-941) -- over host memory (staged through page-locked
+buffers) or device memory (used in place), validated the same way and
+leaving the same bytes in the destination. The native worker admits requests in
 arrival order against the device budget, runs each admitted group as one
 batch launch, and overlaps copies and kernels of successive launches.
 """
@@ -18,14 +19,13 @@ from .ops import _fid
 
 
 def _host(x) -> tuple[int, int, object]:
-    """(address, byte length, owner) of a host buffer: numpy array, CPU
-    torch tensor (page-locked ones are copied without staging), bytearray or
-    (address, length)."""
+    """(address, byte length, owner) of a request buffer: numpy array, torch
+    tensor (page-locked CPU tensors are copied without staging; CUDA tensors
+    on the server's device are used in place), bytearray or (address,
+    length). A request's buffers are all host memory or all device memory."""
     if isinstance(x, tuple):
         return int(x[0]), int(x[1]), None
     if hasattr(x, "data_ptr"):
-        if x.is_cuda:
-            raise TypeError("fgf_b200.serve: request buffers are host memory")
         if not x.is_contiguous():
             raise TypeError("fgf_b200.serve: buffers must be contiguous")
         return int(x.data_ptr()), int(x.numel() * x.element_size()), x
@@ -60,7 +60,7 @@ class PreparedRequest:
 
 
 class Server:
-    """`fgfc_server`: continuous batching over host buffers.
+    """`fgfc_server`: continuous batching of requests over host or device buffers.
 
     `plain=True` serves one request at a time through the per-call entry
     points (the one-call-per-stripe comparison)."""
@@ -76,7 +76,7 @@ class Server:
 
     def submit(self, field, coeffs: Sequence[int], srcs: Sequence, dst, row_len: int, nrows: int,
                overwrite: bool = True, row_starts: Sequence[int] | None = None) -> int:
-        """Enqueue one call; the host buffers must stay untouched until it completes."""
+        """Enqueue one call; its buffers must stay untouched until it completes."""
         return self.submit_prepared(PreparedRequest(field, coeffs, srcs, dst, row_len, nrows, overwrite,
                                                     row_starts))
 

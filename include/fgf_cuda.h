@@ -287,7 +287,7 @@ fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job *job
 
 /* ---------------------------------------------------------------- serving loop */
 
-/* A request loop over HOST buffers. No counterpart in the reference (whose
+/* A request loop over host or device buffers. No counterpart in the reference (whose
  * callers run one `ops` call per stripe on the CPU); each request is exactly
  * one such call -- dot_product_matrix (overwrite), mul_add_matrix
  * (accumulate) or mul_add_matrix_scattered (row_starts != NULL) -- with the
@@ -301,8 +301,10 @@ fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job *job
  * launches overlap on three streams. Coefficient matrices are turned into
  * device plans once and cached, keyed by a hash of (field, dimensions,
  * coefficients). Request buffers in page-locked host memory with rows of at
- * least 256 KiB are copied directly; all others go through the server's
- * page-locked staging buffers. */
+ * least 256 KiB are copied directly; other host buffers go through the
+ * server's page-locked staging buffers. A request whose buffers are all
+ * device memory of the server's device runs in place, without copies (a
+ * request mixing host and device buffers is rejected with FGFC_ERR_ARG). */
 typedef struct fgfc_server fgfc_server;
 
 typedef struct fgfc_server_config {
@@ -341,6 +343,8 @@ typedef struct fgfc_server_stats {
   uint64_t max_batch_seen;
   double p50_us, p99_us, mean_us, max_us; /* submit -> result in host memory */
   double busy_s;         /* first submit -> last completion since the last reset */
+  double queue_us;       /* mean submit -> issue (waiting for admission) */
+  double launch_us;      /* mean issue -> retire of a launch (copies, kernels, completion) */
 } fgfc_server_stats;
 
 fgfc_status fgfc_server_create(const fgfc_server_config *cfg, fgfc_server **out);

@@ -106,11 +106,11 @@ def test_batch_graph_replay_uses_fresh_descriptors(cuda):
                    outs[s * m * rl:(s + 1) * m * rl], rl, m, True) for s in range(nst)]
     b = fb.Batch(graphs=True)
     prep = b.prepare(jobs)
-    for rnd in range(3):
+    for rnd in range(6):
         data = noise(nst * k * rl, 0x52 + rnd)
         srcs.copy_(torch.from_numpy(data).cuda())
         b.run_prepared(prep)
-        if rnd >= 2:
+        if rnd >= 4:  # each of the 4 descriptor slots captures once, then replays
             assert b.stats()["graph_replayed"]
         got = h(outs)
         for s in range(nst):

@@ -163,3 +163,32 @@ def test_limits_validation_and_trivial_requests(cuda):
         dst = np.full(30, 0x5A, np.uint8)
         srv.wait(srv.submit(Gf8D, [], [], dst, 10, 3, overwrite=False))  # accumulate of nothing
         assert (dst == 0x5A).all()
+
+
+def test_device_resident_requests_run_in_place(cuda):
+    """Requests whose shards are already in device memory: no copies, same
+    bytes as the oracle, alone, in the mix and in plain mode."""
+    cases = _cases(5)[1:]
+    for plain in (False, True):
+        with serve.Server(hbm_budget=64 << 20, staging_bytes=16 << 20, plain=plain) as srv:
+            for mode in ("alone", "mix"):
+                dsrcs = [[torch.from_numpy(v.copy()).cuda() for _, v in c.srcs] for c in cases]
+                dsts = [torch.from_numpy(c.init.copy()).cuda() for c in cases]
+                tickets = []
+                for c, ss, dd in zip(cases, dsrcs, dsts):
+                    t = srv.submit(c.field, c.coeffs, ss, dd, c.rl, c.m, overwrite=c.kind == "dot",
+                                   row_starts=c.starts)
+                    if mode == "alone":
+                        srv.wait(t)
+                    else:
+                        tickets.append(t)
+                for t in tickets:
+                    srv.wait(t)
+                for i, (c, dd) in enumerate(zip(cases, dsts)):
+                    assert np.array_equal(dd.cpu().numpy(), c.want), (plain, mode, i)
+            st = srv.stats()
+            assert st["peak_device_bytes"] == 0  # nothing was staged on the server's arena
+    with serve.Server(hbm_budget=64 << 20, staging_bytes=16 << 20) as srv:
+        with pytest.raises(FgfError) as e:
+            srv.submit(Gf8D, [1], [torch.zeros(64, dtype=torch.uint8, device="cuda")], np.zeros(64, np.uint8), 64, 1)
+        assert e.value.status == 11
