@@ -159,6 +159,8 @@ _SIGS = {
                                                  C.POINTER(Term), c_size, c_stream]),
     "fgfc_mul_add_matrix_scattered_with": (c_status, [c_u8p, c_size, c_size, C.POINTER(c_size), c_size,
                                                       C.c_void_p, C.POINTER(Slice), c_size, c_stream]),
+    "fgfc_dot_product_matrix_scattered_with": (c_status, [c_u8p, c_size, c_size, C.POINTER(c_size), c_size,
+                                                          C.c_void_p, C.POINTER(Slice), c_size, c_stream]),
     "fgfc_batch_create": (c_status, [C.POINTER(C.c_void_p)]),
     "fgfc_batch_destroy": (None, [C.c_void_p]),
     "fgfc_batch_set_graphs": (c_status, [C.c_void_p, C.c_int]),
@@ -166,6 +168,13 @@ _SIGS = {
     "fgfc_batch_stats": (c_status, [C.c_void_p, C.POINTER(c_size), C.POINTER(c_size), C.POINTER(C.c_int)]),
     "fgfc_batch_run_noalloc": (c_status, [C.c_int, C.POINTER(NoAllocJob), c_size, c_stream]),
     "fgfc_run_jobs_serial": (c_status, [C.POINTER(MatrixJob), c_size, c_stream]),
+    "fgfc_tune_force": (c_status, [C.c_int]),
+    "fgfc_tune_choice": (C.c_int, [C.c_int, c_size, c_size, c_size]),
+    "fgfc_tune_usable": (C.c_int, [C.c_int, C.c_int, c_size, c_size]),
+    "fgfc_tune_shape": (c_status, [C.c_int, c_size, c_size, c_size, C.POINTER(C.c_int)]),
+    "fgfc_tune_save": (c_status, [C.c_char_p]),
+    "fgfc_tune_load": (c_status, [C.c_char_p]),
+    "fgfc_tune_clear": (None, []),
     "fgfc_server_create": (c_status, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "fgfc_server_submit": (c_status, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
     "fgfc_server_wait": (c_status, [C.c_void_p, C.c_uint64]),

@@ -27,7 +27,7 @@ class Job:
     row_len: int
     nrows: int
     overwrite: bool = True
-    row_starts: Sequence[int] | None = None  # scattered rows (accumulate only)
+    row_starts: Sequence[int] | None = None  # scattered rows (overwrite: zero-then-accumulate in one pass)
 
 
 class Prepared:

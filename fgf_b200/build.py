@@ -1,5 +1,9 @@
 """Build libfgfcuda.so in-tree (sm_100a) and the oracle's C library.
 
+Each translation unit is compiled to an object in parallel (the kernels are
+self-contained per file, so no relocatable device code is needed), then the
+objects are linked into one shared library.
+
 Usage: python -m fgf_b200.build [--force]
 """
 from __future__ import annotations
@@ -7,16 +11,20 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
+OBJ = PKG / "_build"
 LIB = PKG / "libfgfcuda.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["kernels.cu", "batch.cu", "api.cpp", "tables.cpp", "serve.cpp"]
+SOURCES = ["kernels.cu", "batch.cu", "gf2mma.cu", "api.cpp", "tables.cpp", "serve.cpp", "decode.cpp",
+           "tune.cpp"]
+FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 
 
 def _stale(out: Path, deps: list[Path]) -> bool:
@@ -26,14 +34,25 @@ def _stale(out: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps if d.exists())
 
 
+def _compile(src: Path, headers: list[Path], force: bool, verbose: bool) -> Path:
+    obj = OBJ / (src.name + ".o")
+    if force or _stale(obj, [src, *headers]):
+        cmd = [NVCC, *FLAGS, "-c", "-o", str(obj), str(src)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, cwd=CSRC)
+    return obj
+
+
 def build_lib(force: bool = False, verbose: bool = False) -> Path:
     srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
-    deps = srcs + list(CSRC.glob("*.hpp")) + [ROOT / "include" / "fgf_cuda.h"]
-    if not force and not _stale(LIB, deps):
+    headers = list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "fgf_cuda.h"]
+    if not force and not _stale(LIB, srcs + headers):
         return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-           "-cudart", "static", "-Xptxas", "-warn-spills", "-o", str(LIB), *map(str, srcs),
-           "-lpthread"]
+    OBJ.mkdir(exist_ok=True)
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, headers, force, verbose), srcs))
+    cmd = [NVCC, *ARCH, "--shared", "-cudart", "static", "-o", str(LIB), *map(str, objs), "-lpthread"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=CSRC)

@@ -135,6 +135,7 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
     for (size_t j = 0; j < m; ++j) shift |= (reinterpret_cast<uintptr_t>(rows[j]) & 15) != al;
   }
 
+  const bool byte_tables = choose_kernel(field, k, m, len) == FGFC_KERNEL_BYTE;
   static thread_local MatrixLaunch a;  // large (inline tables): keep off the stack
   for (size_t g0 = 0; g0 < gtot; g0 += gp) {
     const size_t G = std::min(gp, gtot - g0);
@@ -165,7 +166,7 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
       cudaError_t e;
       {
         std::lock_guard<std::mutex> lk(g_launch_mu);
-        e = launch_matrix(field, static_cast<int>(G), overwrite && t0 == 0, a, stream);
+        e = launch_matrix(field, static_cast<int>(G), overwrite && t0 == 0, a, stream, byte_tables);
       }
       if (e != cudaSuccess) return cuda_fail(e, name);
     }
@@ -772,11 +773,10 @@ fgfc_status fgfc_mul_add_matrix_scattered(fgfc_field field, uint8_t* dst, size_t
   return run_matrix(field, sp.data(), nterms, rp.data(), nrows, cs, row_len, false, stream, name);
 }
 
-fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t* dst, size_t dst_len, size_t row_len,
-                                               const size_t* row_starts, size_t nrows,
-                                               const fgfc_plan* plan, const fgfc_slice* srcs,
-                                               size_t nsrcs, fgfc_stream stream) {
-  const char* name = "mul_add_matrix_scattered_with";
+static fgfc_status scattered_plan_impl(const char* name, bool overwrite, uint8_t* dst, size_t dst_len,
+                                       size_t row_len, const size_t* row_starts, size_t nrows,
+                                       const fgfc_plan* plan, const fgfc_slice* srcs, size_t nsrcs,
+                                       fgfc_stream stream) {
   fgfc_status st;
   if (!plan) return fail(FGFC_ERR_ARG, "%s: null plan", name);
   if (!check_scattered_rows(plan->field, name, dst_len, row_len, row_starts, nrows, &st)) return st;
@@ -787,13 +787,29 @@ fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t* dst, size_t dst_len, siz
     if (srcs[i].len != row_len)
       return fail(FGFC_ERR_SOURCE, "%s: source %zu is %zu bytes, expected %zu", name, i, srcs[i].len,
                   row_len);
-  if (nrows == 0 || nsrcs == 0) return ok();
+  if (nrows == 0 || (nsrcs == 0 && !overwrite)) return ok();
   std::vector<const uint8_t*> sp(nsrcs);
   for (size_t i = 0; i < nsrcs; ++i) sp[i] = srcs[i].ptr;
   std::vector<uint8_t*> rp(nrows);
   for (size_t j = 0; j < nrows; ++j) rp[j] = dst + row_starts[j];
-  return run_matrix(plan->field, sp.data(), nsrcs, rp.data(), nrows, plan_mat(plan), row_len, false,
+  return run_matrix(plan->field, sp.data(), nsrcs, rp.data(), nrows, plan_mat(plan), row_len, overwrite,
                     stream, name);
+}
+
+fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t* dst, size_t dst_len, size_t row_len,
+                                               const size_t* row_starts, size_t nrows,
+                                               const fgfc_plan* plan, const fgfc_slice* srcs,
+                                               size_t nsrcs, fgfc_stream stream) {
+  return scattered_plan_impl("mul_add_matrix_scattered_with", false, dst, dst_len, row_len, row_starts, nrows,
+                             plan, srcs, nsrcs, stream);
+}
+
+fgfc_status fgfc_dot_product_matrix_scattered_with(uint8_t* dst, size_t dst_len, size_t row_len,
+                                                   const size_t* row_starts, size_t nrows,
+                                                   const fgfc_plan* plan, const fgfc_slice* srcs,
+                                                   size_t nsrcs, fgfc_stream stream) {
+  return scattered_plan_impl("dot_product_matrix_scattered_with", true, dst, dst_len, row_len, row_starts,
+                             nrows, plan, srcs, nsrcs, stream);
 }
 
 }  // extern "C"
@@ -887,15 +903,14 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
   low.reserve(njobs);
   for (size_t i = 0; i < njobs; ++i) {
     const fgfc_matrix_job& J = jobs[i];
-    const char* name = J.row_starts ? "mul_add_matrix_scattered_with"
+    const char* name = J.row_starts ? (J.overwrite ? "dot_product_matrix_scattered_with"
+                                                   : "mul_add_matrix_scattered_with")
                                     : (J.overwrite ? "dot_product_matrix_with" : "mul_add_matrix_with");
     fgfc_status st;
     const fgfc_plan* plan = J.plan;
     if (!plan) return fail(FGFC_ERR_ARG, "batch job %zu: %s: null plan", i, name);
     const int field = plan->field;
     if (J.row_starts) {
-      if (J.overwrite)
-        return fail(FGFC_ERR_ARG, "batch job %zu: scattered rows accumulate; overwrite is not defined", i);
       if (!check_scattered_rows(field, name, J.dst_len, J.row_len, J.row_starts, J.nrows, &st)) {
         t_err = "batch job " + std::to_string(i) + ": " + t_err;
         return st;
@@ -922,9 +937,12 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
                     J.srcs[t].len, J.row_len);
     if (J.nrows == 0 || J.row_len == 0) continue;
     if (J.nsrcs == 0) {
-      if (J.overwrite) {
-        cudaError_t e = cudaMemsetAsync(J.dst, 0, J.nrows * J.row_len, stream);
-        if (e != cudaSuccess) return cuda_fail(e, name);
+      if (J.overwrite) {  // an empty sum overwrites with zero
+        for (size_t j = 0; j < J.nrows; ++j) {
+          cudaError_t e =
+              cudaMemsetAsync(J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len), 0, J.row_len, stream);
+          if (e != cudaSuccess) return cuda_fail(e, name);
+        }
       }
       continue;
     }
@@ -945,10 +963,10 @@ fgfc_status fgfc_run_jobs_serial(const fgfc_matrix_job* jobs, size_t njobs, fgfc
     const fgfc_matrix_job& J = jobs[i];
     fgfc_status st;
     if (J.row_starts) {
-      if (J.overwrite)
-        return fail(FGFC_ERR_ARG, "batch job %zu: scattered rows accumulate; overwrite is not defined", i);
-      st = fgfc_mul_add_matrix_scattered_with(J.dst, J.dst_len, J.row_len, J.row_starts, J.nrows, J.plan, J.srcs,
-                                              J.nsrcs, stream);
+      st = J.overwrite ? fgfc_dot_product_matrix_scattered_with(J.dst, J.dst_len, J.row_len, J.row_starts,
+                                                                J.nrows, J.plan, J.srcs, J.nsrcs, stream)
+                       : fgfc_mul_add_matrix_scattered_with(J.dst, J.dst_len, J.row_len, J.row_starts, J.nrows,
+                                                            J.plan, J.srcs, J.nsrcs, stream);
     } else if (J.overwrite) {
       st = fgfc_dot_product_matrix_with(J.dst, J.dst_len, J.row_len, J.nrows, J.plan, J.srcs, J.nsrcs, stream);
     } else {
@@ -1028,7 +1046,6 @@ fgfc_status validate_matrix_call(int field, const char* name, size_t dst_len, si
   fgfc_status st;
   if (!valid_field(field)) return fail(FGFC_ERR_ARG, "%s: unknown field", name);
   if (row_starts) {
-    if (overwrite) return fail(FGFC_ERR_ARG, "%s: scattered rows accumulate; overwrite is not defined", name);
     if (!check_scattered_rows(field, name, dst_len, row_len, row_starts, nrows, &st)) return st;
   } else {
     if (!check_width(field, name, row_len, &st)) return st;

@@ -765,8 +765,6 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
   uparams.clear();
   std::string key = std::to_string(reinterpret_cast<uintptr_t>(s.dev)) + ":" + std::to_string(bytes);
   const int sms = sm_count();
-  static std::mutex attr_mu;
-  static bool attr_set[1024] = {false};
   size_t ci = 0;
   for (auto& kv : classes) {
     const BatchClass& c = kv.second;
@@ -782,15 +780,9 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     if (!L.fn && !L.ufn) return cudaErrorInvalidValue;
     L.smem = fast ? fast_smem(c.K) : static_cast<uint32_t>(kBatchSmem);
     L.threads = fast ? static_cast<unsigned>(kFastThreads) : static_cast<unsigned>(kThreads);
-    {
-      std::lock_guard<std::mutex> lk2(attr_mu);
-      if (!attr_set[akey]) {
-        e = L.ufn ? cudaFuncSetAttribute(L.ufn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.smem))
-                  : cudaFuncSetAttribute(L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L.smem));
-        if (e != cudaSuccess) return e;
-        attr_set[akey] = true;
-      }
-    }
+    e = ensure_smem_attr(L.ufn ? reinterpret_cast<const void*>(L.ufn) : reinterpret_cast<const void*>(L.fn),
+                         static_cast<int>(L.smem));
+    if (e != cudaSuccess) return e;
     if (c.uniform) {
       // one launch per block of kUniformJobs stripes
       for (size_t q0 = 0; q0 < c.jobs.size(); q0 += kUniformJobs) {
@@ -922,12 +914,24 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
 
 // ---------------------------------------------------------------- without allocation
 //
-// fgfc_batch_run_noalloc: the work-list kernel above, with every byte of
-// scratch it needs (descriptors, pointers, work items, the claim counter and
+// fgfc_batch_run_noalloc: the work-list kernels above, with every byte of
+// scratch they need (descriptors, pointers, work items, the claim counters and
 // the stripes' compact product tables) placed in this fixed device array
 // instead of device memory allocated for the call. The host side builds the
 // whole blob in a fixed host array of the same size and copies it in with one
 // stream-ordered copy, so nothing is allocated on either side.
+//
+// The host array is pageable, so the runtime stages the copy before the call
+// returns: the call may block the host until the stream reaches the copy, and
+// that is also what makes it safe to refill the host array on the next call.
+// (Pinning the array would make the copy truly asynchronous, but then every
+// call would first have to wait on an event recorded after the previous copy.)
+//
+// Stripes are grouped in classes as in fgfc_batch_run: Gf8 stripes of at most
+// 4 rows and at most 14 sources run the byte-table kernel for their source
+// count; the rest run the split-nibble kernel for their own number of table
+// groups, so a wide stripe does not widen the others. One launch per class,
+// in order, on the caller's stream.
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[FGFC_NOALLOC_SCRATCH_BYTES];
 alignas(256) static uint8_t g_noalloc_host[FGFC_NOALLOC_SCRATCH_BYTES];
@@ -935,12 +939,37 @@ static std::mutex g_noalloc_mu;
 constexpr int kNoallocMaxDevices = 64;
 static uint8_t* g_noalloc_dev[kNoallocMaxDevices];  // device address of the array, per device
 
+namespace {
+
+// Class of a stripe in fgfc_batch_run_noalloc: 1..14 = byte-table kernel
+// with that many sources, 100 + G = nibble kernel with G table groups.
+int noalloc_class(int E, size_t nsrcs, size_t nrows) {
+  const int R = 4 / E;
+  const size_t G = (nrows + R - 1) / R;
+  if (E == 1 && G == 1 && nsrcs >= 1 && nsrcs <= static_cast<size_t>(kFastMaxK)) return static_cast<int>(nsrcs);
+  return 100 + static_cast<int>(G);
+}
+
+}  // namespace
+
 // Returns 0, or an fgfc_status-style code with `msg` filled in.
 int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStream_t stream, char* msg,
                 size_t msglen) {
+  // A graph recorded from this call would replay whatever the shared host
+  // and device arrays hold at replay time, not this call's descriptors.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) {
+    snprintf(msg, msglen, "batch_run_noalloc: %s", cudaGetErrorString(e));
+    return FGFC_ERR_CUDA;
+  }
+  if (cap != cudaStreamCaptureStatusNone) {
+    snprintf(msg, msglen, "batch_run_noalloc: the stream is being captured; this call cannot be recorded");
+    return FGFC_ERR_ARG;
+  }
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
     snprintf(msg, msglen, "batch_run_noalloc: no usable current device");
     return FGFC_ERR_CUDA;
@@ -960,8 +989,10 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
   const int E = field_bytes(field);
   const int R = 4 / E;
 
-  // ---- sizes (one class: every stripe uses G table groups)
-  size_t G = 1, nptr = 0, ntab = 0, nitems = 0, nlive = 0;
+  // ---- sizes: per class its items; every stripe's tables at its own G
+  constexpr int kClasses = 105;  // byte-table 1..14, nibble 101..104
+  size_t nptr = 0, ntab = 0, nlive = 0;
+  size_t class_items[kClasses] = {0};
   for (size_t i = 0; i < njobs; ++i) {
     const fgfc_noalloc_job& J = jobs[i];
     if (J.nrows == 0 || J.row_len == 0 || J.nsrcs == 0) continue;
@@ -970,23 +1001,28 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
                i, J.nrows, J.nsrcs, 4 * R, kMaxSrc);
       return FGFC_ERR_LIMIT;
     }
-    G = std::max<size_t>(G, (J.nrows + R - 1) / R);
-  }
-  for (size_t i = 0; i < njobs; ++i) {
-    const fgfc_noalloc_job& J = jobs[i];
-    if (J.nrows == 0 || J.row_len == 0 || J.nsrcs == 0) continue;
+    const size_t G = (J.nrows + R - 1) / R;
+    const int cls = noalloc_class(E, J.nsrcs, J.nrows);
+    const bool fast = cls < 100;
     ++nlive;
     nptr += J.nsrcs + J.nrows;
     ntab += J.nsrcs * E * G * kCompactWords;
     const uint64_t nvec = J.row_len / 16 + 1;  // upper bound before alignment is known
-    nitems += (nvec + kVecPerItem - 1) / kVecPerItem + (J.row_len / 4 + 2 + kGroupsPerItem - 1) / kGroupsPerItem + 1;
+    const uint64_t per_vec = fast ? kFastVecPerItem : kVecPerItem;
+    const uint64_t per_grp = fast ? kFastGroupsPerItem : kGroupsPerItem;
+    class_items[cls] += (nvec + per_vec - 1) / per_vec + (J.row_len / 4 + 2 + per_grp - 1) / per_grp + 1;
   }
   const size_t off_jobs = 0;
   const size_t off_ptrs = align16(off_jobs + nlive * sizeof(BatchJob));
   const size_t off_tabs = align16(off_ptrs + nptr * sizeof(uint64_t));
-  const size_t off_items = align16(off_tabs + ntab * sizeof(uint32_t));
-  const size_t off_counter = align16(off_items + nitems * sizeof(uint2));
-  const size_t bytes = off_counter + 64;
+  size_t class_off[kClasses] = {0};
+  size_t off = align16(off_tabs + ntab * sizeof(uint32_t));
+  for (int c = 0; c < kClasses; ++c) {
+    if (!class_items[c]) continue;
+    class_off[c] = off;  // items, then a 64-byte counter
+    off = align16(off + class_items[c] * sizeof(uint2)) + 64;
+  }
+  const size_t bytes = off;
   if (bytes > FGFC_NOALLOC_SCRATCH_BYTES) {
     snprintf(msg, msglen, "batch_run_noalloc: submission needs %zu bytes of scratch, more than the %u available",
              bytes, static_cast<unsigned>(FGFC_NOALLOC_SCRATCH_BYTES));
@@ -997,8 +1033,8 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
   BatchJob* hj = reinterpret_cast<BatchJob*>(g_noalloc_host + off_jobs);
   uint64_t* hp = reinterpret_cast<uint64_t*>(g_noalloc_host + off_ptrs);
   uint32_t* ht = reinterpret_cast<uint32_t*>(g_noalloc_host + off_tabs);
-  uint2* hi = reinterpret_cast<uint2*>(g_noalloc_host + off_items);
-  size_t jn = 0, pn = 0, tn = 0, in = 0;
+  size_t jn = 0, pn = 0, tn = 0;
+  size_t class_n[kClasses] = {0};
   for (size_t i = 0; i < njobs; ++i) {
     const fgfc_noalloc_job& S = jobs[i];
     if (S.nrows == 0 || S.row_len == 0) continue;
@@ -1014,6 +1050,9 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
       }
       continue;
     }
+    const size_t G = (S.nrows + R - 1) / R;
+    const int cls = noalloc_class(E, S.nsrcs, S.nrows);
+    const bool fast = cls < 100;
     BatchJob& J = hj[jn];
     const uintptr_t al = reinterpret_cast<uintptr_t>(S.srcs[0].ptr) & 15;
     bool same = (al % E) == 0;
@@ -1046,30 +1085,45 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
     J.k = static_cast<uint32_t>(S.nsrcs);
     J.nrows = static_cast<uint32_t>(S.nrows);
     J.ovr = S.overwrite ? 1u : 0u;
-    const uint64_t nv_items = (J.nvec + kVecPerItem - 1) / kVecPerItem;
+    const uint64_t per_vec = fast ? kFastVecPerItem : kVecPerItem;
+    const uint64_t per_grp = fast ? kFastGroupsPerItem : kGroupsPerItem;
+    const uint64_t nv_items = (J.nvec + per_vec - 1) / per_vec;
     const uint64_t tail = J.len - J.head - 16 * J.nvec;
-    const uint64_t ns_items = ((J.head + 3) / 4 + (tail + 3) / 4 + kGroupsPerItem - 1) / kGroupsPerItem;
+    const uint64_t ns_items = ((J.head + 3) / 4 + (tail + 3) / 4 + per_grp - 1) / per_grp;
     J.nv_items = static_cast<uint32_t>(nv_items);
-    for (uint64_t q = 0; q < nv_items + ns_items; ++q) hi[in++] = make_uint2(static_cast<unsigned>(jn), static_cast<unsigned>(q));
+    uint2* hi = reinterpret_cast<uint2*>(g_noalloc_host + class_off[cls]);
+    for (uint64_t q = 0; q < nv_items + ns_items; ++q)
+      hi[class_n[cls]++] = make_uint2(static_cast<unsigned>(jn), static_cast<unsigned>(q));
     ++jn;
   }
-  if (jn == 0 || in == 0) return 0;
-  std::memset(g_noalloc_host + off_counter, 0, 64);  // the claim counter starts at zero every call
+  if (jn == 0) return 0;
+  for (int c = 0; c < kClasses; ++c)  // every claim counter starts at zero on every call
+    if (class_items[c]) std::memset(g_noalloc_host + align16(class_off[c] + class_items[c] * sizeof(uint2)), 0, 64);
 
-  // ---- one copy, one launch of the work-list kernel on the scratch
+  // ---- one copy, then one launch of the work-list kernel per class
   e = cudaMemcpyAsync(dbase, g_noalloc_host, bytes, cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) {
-    KernelFn fn = kernel_for(E, static_cast<int>(G), false);  // rows share the sources' alignment here
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kBatchSmem));
-    if (e == cudaSuccess) {
-      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((in + kClaim - 1) / kClaim, sm_count()));
-      fn<<<grid, kThreads, kBatchSmem, stream>>>(reinterpret_cast<const BatchJob*>(dbase + off_jobs),
-                                                 reinterpret_cast<const uint64_t*>(dbase + off_ptrs),
-                                                 reinterpret_cast<const uint2*>(dbase + off_items),
-                                                 static_cast<uint32_t>(in),
-                                                 reinterpret_cast<uint32_t*>(dbase + off_counter));
-      e = cudaGetLastError();
+  for (int c = 0; c < kClasses && e == cudaSuccess; ++c) {
+    if (!class_n[c]) continue;
+    const bool fast = c < 100;
+    // rows share the sources' alignment here (otherwise the whole stripe is scalar)
+    KernelFn fn = fast ? fast_kernel_for(c, false) : kernel_for(E, c - 100, false);
+    const int smem = fast ? static_cast<int>(fast_smem(c)) : static_cast<int>(kBatchSmem);
+    const unsigned threads = fast ? static_cast<unsigned>(kFastThreads) : static_cast<unsigned>(kThreads);
+    if (!fn) {
+      e = cudaErrorInvalidValue;
+      break;
     }
+    e = ensure_smem_attr(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) break;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((class_n[c] + kClaim - 1) / kClaim, sm_count()));
+    const size_t items_off = class_off[c];
+    const size_t counter_off = align16(class_off[c] + class_items[c] * sizeof(uint2));
+    fn<<<grid, threads, smem, stream>>>(reinterpret_cast<const BatchJob*>(dbase + off_jobs),
+                                        reinterpret_cast<const uint64_t*>(dbase + off_ptrs),
+                                        reinterpret_cast<const uint2*>(dbase + items_off),
+                                        static_cast<uint32_t>(class_n[c]),
+                                        reinterpret_cast<uint32_t*>(dbase + counter_off));
+    e = cudaGetLastError();
   }
   if (e != cudaSuccess) {
     snprintf(msg, msglen, "batch_run_noalloc: CUDA error: %s", cudaGetErrorString(e));

@@ -53,8 +53,10 @@ void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0
 
 // Kernel entry (kernels.cu). `groups` = G for this launch; `overwrite`
 // selects dot-product (overwrite) or mul_add (accumulate) semantics.
+// `byte_tables`: run the byte-table kernel (Gf8, one group, <= 14 sources)
+// for the vector body instead of the split-nibble kernel.
 cudaError_t launch_matrix(int field, int groups, bool overwrite, const MatrixLaunch& a,
-                          cudaStream_t s);
+                          cudaStream_t s, bool byte_tables);
 // Fill `n` rows of `len` bytes with zero.
 cudaError_t launch_zero_rows(uint8_t* const* rows, int n, uint64_t len, cudaStream_t s);
 // dst ^= src over `len` bytes.
@@ -64,6 +66,17 @@ cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const 
                                uint64_t len, cudaStream_t s);
 
 int sm_count();
+
+// Kernel families (fgfc_kernel values) and the choice per shape (tune.cpp).
+constexpr size_t kFastMaxSources = 14;  // byte-table kernels: sources per launch
+bool kernel_usable(int kernel, int field, size_t k, size_t m);
+int choose_kernel(int field, size_t k, size_t m, size_t len);
+// Shapes the bit-sliced tensor-core contraction covers in one launch
+// (gf2mma.cu): at most 512 input bits and 128 output bits per element column.
+bool gf2mma_shape_ok(int field, size_t k, size_t m);
+// Opt `fn` in to `bytes` of dynamic shared memory on the current device, once
+// per (device, kernel); thread-safe.
+cudaError_t ensure_smem_attr(const void* fn, int bytes);
 
 // One lowered sub-job of a batched submission: all sources of a stripe and
 // the rows of at most 4 table groups, with its alignment split resolved.

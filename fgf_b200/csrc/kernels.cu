@@ -19,7 +19,11 @@
 // (src/kernel/x86/gf8.rs:2208-2315), and is written once.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "fast_core.cuh"
 #include "internal.hpp"
@@ -224,9 +228,8 @@ __global__ void __launch_bounds__(256) matrix_scalar_kernel(const __grid_constan
 // ---------------------------------------------------------------- byte-table kernel
 //
 // Gf8, at most 4 rows, K <= 14 sources: the RS(10,4) encode / reconstruct
-// shape and the single-row ops (fast_core.cuh). Rows shorter than
-// kFastMinVec vectors use the nibble kernel, whose tables fill faster.
-constexpr uint64_t kFastMinVec = 1u << 18;  // 4 MiB
+// shape and the single-row ops (fast_core.cuh). Chosen per call by the tuner
+// (tune.cpp): short rows use the nibble kernel, whose tables fill faster.
 
 template <int K, bool OVR, bool SHIFT>
 __global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __grid_constant__ MatrixLaunch a) {
@@ -264,18 +267,11 @@ __global__ void __launch_bounds__(kFastThreads, 1) matrix_fast_kernel(const __gr
   }
 }
 
-int g_sms = 0;
-
 template <int K, bool OVR, bool SHIFT>
 cudaError_t launch_fast_k(const MatrixLaunch& a, cudaStream_t s) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(matrix_fast_kernel<K, OVR, SHIFT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         FastLayout<K>::smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(matrix_fast_kernel<K, OVR, SHIFT>),
+                                   FastLayout<K>::smem);
+  if (e != cudaSuccess) return e;
   const uint64_t want = (a.nvec + kFastThreads - 1) / kFastThreads;
   const uint64_t cap = static_cast<uint64_t>(sm_count());
   const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
@@ -310,26 +306,17 @@ cudaError_t launch_fast(const MatrixLaunch& a, cudaStream_t s) {
 }
 
 template <int E, int G, bool OVR>
-cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
-  static bool configured = false;
-  static int occ_vec = 1;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kMaxSlots * (kSlotBytes + kCompactWords * 4));
+cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s, bool byte_tables) {
+  constexpr int kSmemMax = kMaxSlots * (kSlotBytes + kCompactWords * 4);
+  for (const void* fn : {reinterpret_cast<const void*>(matrix_vec_kernel<E, G, OVR, false>),
+                         reinterpret_cast<const void*>(matrix_vec_kernel<E, G, OVR, true>),
+                         reinterpret_cast<const void*>(matrix_scalar_kernel<E, G, OVR>)}) {
+    cudaError_t e = ensure_smem_attr(fn, kSmemMax);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(matrix_vec_kernel<E, G, OVR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kMaxSlots * (kSlotBytes + kCompactWords * 4));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(matrix_scalar_kernel<E, G, OVR>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kMaxSlots * (kSlotBytes + kCompactWords * 4));
-    if (e != cudaSuccess) return e;
-    configured = true;
   }
   const size_t smem = static_cast<size_t>(a.k) * E * G * (kSlotBytes + kCompactWords * 4);
   const int sms = sm_count();
-  if (E == 1 && G == 1 && a.k <= 14 && a.nvec >= kFastMinVec) {
+  if (E == 1 && G == 1 && a.k <= 14 && a.nvec && byte_tables) {
     cudaError_t e = launch_fast<OVR>(a, s);
     if (e != cudaSuccess) return e;
   } else if (a.nvec) {
@@ -337,7 +324,7 @@ cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
     auto kern = a.shift ? matrix_vec_kernel<E, G, OVR, true> : matrix_vec_kernel<E, G, OVR, false>;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 512, smem);
     if (e != cudaSuccess) return e;
-    occ_vec = occ > 0 ? occ : 1;
+    const int occ_vec = occ > 0 ? occ : 1;
     uint64_t want = (a.nvec + 511) / 512;
     uint64_t cap = static_cast<uint64_t>(sms) * occ_vec;
     const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
@@ -363,12 +350,12 @@ cudaError_t launch_one(const MatrixLaunch& a, cudaStream_t s) {
 }
 
 template <int E, bool OVR>
-cudaError_t launch_e(int groups, const MatrixLaunch& a, cudaStream_t s) {
+cudaError_t launch_e(int groups, const MatrixLaunch& a, cudaStream_t s, bool bt) {
   switch (groups) {
-    case 1: return launch_one<E, 1, OVR>(a, s);
-    case 2: return launch_one<E, 2, OVR>(a, s);
-    case 3: return launch_one<E, 3, OVR>(a, s);
-    case 4: return launch_one<E, 4, OVR>(a, s);
+    case 1: return launch_one<E, 1, OVR>(a, s, bt);
+    case 2: return launch_one<E, 2, OVR>(a, s, bt);
+    case 3: return launch_one<E, 3, OVR>(a, s, bt);
+    case 4: return launch_one<E, 4, OVR>(a, s, bt);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -398,7 +385,10 @@ __global__ void xor_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict_
 
 __constant__ uint8_t c_exp[2][512];
 __constant__ uint8_t c_log[2][256];
-bool g_const_ready = false;
+// __constant__ memory is per device: the tables are uploaded once per device.
+constexpr int kMaxDevices = 64;
+std::atomic<bool> g_const_ready[kMaxDevices];
+std::mutex g_const_mu;
 
 __device__ __forceinline__ uint8_t emul(const uint8_t* ex, const uint8_t* lg, uint8_t x, uint8_t y) {
   return (x && y) ? ex[lg[x] + lg[y]] : 0;
@@ -446,21 +436,43 @@ __global__ void elementwise_kernel(uint8_t* dst, const uint8_t* a, const uint8_t
 }  // namespace
 
 int sm_count() {
-  if (!g_sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sms <= 0) g_sms = 148;
-  }
-  return g_sms;
+  static std::atomic<int> sms[kMaxDevices];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const bool cached = dev >= 0 && dev < kMaxDevices;
+  int v = cached ? sms[dev].load(std::memory_order_relaxed) : 0;
+  if (v > 0) return v;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+  if (v <= 0) v = 148;
+  if (cached) sms[dev].store(v, std::memory_order_relaxed);
+  return v;
+}
+
+// cudaFuncSetAttribute acts on the current device only, so the opt-in to
+// more than 48 KiB of dynamic shared memory is recorded per (device, kernel)
+// and taken under a lock: plans, batch runners and servers may target any
+// device from any host thread.
+cudaError_t ensure_smem_attr(const void* fn, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(dev, fn);
+  const auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done[key] = bytes;
+  return e;
 }
 
 cudaError_t launch_matrix(int field, int groups, bool overwrite, const MatrixLaunch& a,
-                          cudaStream_t s) {
+                          cudaStream_t s, bool bt) {
   const int E = field_bytes(field);
-  if (E == 1) return overwrite ? launch_e<1, true>(groups, a, s) : launch_e<1, false>(groups, a, s);
-  if (E == 2) return overwrite ? launch_e<2, true>(groups, a, s) : launch_e<2, false>(groups, a, s);
-  if (E == 4) return overwrite ? launch_e<4, true>(groups, a, s) : launch_e<4, false>(groups, a, s);
+  if (E == 1) return overwrite ? launch_e<1, true>(groups, a, s, bt) : launch_e<1, false>(groups, a, s, bt);
+  if (E == 2) return overwrite ? launch_e<2, true>(groups, a, s, bt) : launch_e<2, false>(groups, a, s, bt);
+  if (E == 4) return overwrite ? launch_e<4, true>(groups, a, s, bt) : launch_e<4, false>(groups, a, s, bt);
   return cudaErrorInvalidValue;
 }
 
@@ -492,7 +504,12 @@ cudaError_t launch_xor(uint8_t* dst, const uint8_t* src, uint64_t len, cudaStrea
 cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
                                uint64_t len, cudaStream_t s) {
   if (!len) return cudaSuccess;
-  if (!g_const_ready) {
+  int dev = 0;
+  cudaError_t de = cudaGetDevice(&dev);
+  if (de != cudaSuccess) return de;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_const_ready[dev].load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> lk(g_const_mu);
     uint8_t ex[2][512], lg[2][256];
     const Gf8Log* t[2] = {&gf8b_tab(), &gf8d_tab()};
     for (int w = 0; w < 2; ++w) {
@@ -503,7 +520,7 @@ cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const 
     if (e != cudaSuccess) return e;
     e = cudaMemcpyToSymbol(c_log, lg, sizeof(lg));
     if (e != cudaSuccess) return e;
-    g_const_ready = true;
+    g_const_ready[dev].store(true, std::memory_order_release);
   }
   const uint64_t nelem = len / field_bytes(field);
   uint64_t want = (nelem + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;

@@ -373,6 +373,17 @@ def mul_add_matrix_scattered_with(dst, row_len: int, row_starts: Sequence[int], 
                                                    ns, _stream(stream)))
 
 
+def dot_product_matrix_scattered_with(dst, row_len: int, row_starts: Sequence[int], plan: Plan,
+                                      srcs: Sequence, stream=None) -> None:
+    """Extension (no reference counterpart): the overwrite form of the
+    scattered op. Equal to zeroing the rows, then mul_add_matrix_scattered."""
+    d, dn = _buf(dst)
+    starts = (C.c_size_t * max(1, len(row_starts)))(*[int(s) for s in row_starts])
+    sl, ns = _slices(srcs)
+    check(lib().fgfc_dot_product_matrix_scattered_with(d, dn, row_len, starts, len(row_starts), plan.handle,
+                                                       sl, ns, _stream(stream)))
+
+
 # ---------------------------------------------------------------- pack / unpack (host)
 
 def pack(field, elems: Sequence[int]) -> bytes:

@@ -194,14 +194,26 @@ fgfc_status fgfc_mul_add_matrix_scattered_with(uint8_t *dst, size_t dst_len, siz
                                                const size_t *row_starts, size_t nrows,
                                                const fgfc_plan *plan, const fgfc_slice *srcs,
                                                size_t nsrcs, fgfc_stream stream);
+/* Extension with no reference counterpart: the overwrite form of the
+ * scattered op, rows[j] at dst + row_starts[j] = sum_t plan(t, j) * srcs[t].
+ * It gives exactly what zeroing the rows and then calling
+ * mul_add_matrix_scattered(_with) gives (the recipe a caller of the reference
+ * uses to rebuild erased shards in place), in one pass that never reads the
+ * rows' prior contents. Same validation as the accumulate form. */
+fgfc_status fgfc_dot_product_matrix_scattered_with(uint8_t *dst, size_t dst_len, size_t row_len,
+                                                   const size_t *row_starts, size_t nrows,
+                                                   const fgfc_plan *plan, const fgfc_slice *srcs,
+                                                   size_t nsrcs, fgfc_stream stream);
 
 /* ---------------------------------------------------------------- batches */
 
 /* One stripe of a batched submission: the arguments of one
- * dot_product_matrix_with (overwrite = 1), mul_add_matrix_with (overwrite =
- * 0, row_starts = NULL) or mul_add_matrix_scattered_with (row_starts set)
- * call (src/ops.rs:720-867, 887-941). Each job is validated exactly as that
- * call would be. */
+ * dot_product_matrix_with (overwrite = 1, row_starts = NULL),
+ * mul_add_matrix_with (overwrite = 0, row_starts = NULL),
+ * mul_add_matrix_scattered_with (overwrite = 0, row_starts set) or
+ * dot_product_matrix_scattered_with (overwrite = 1, row_starts set) call
+ * (src/ops.rs:720-867, 887-941). Each job is validated exactly as that call
+ * would be. */
 typedef struct fgfc_matrix_job {
   const fgfc_plan *plan;    /* dimensions (nsrcs, nrows) */
   const fgfc_slice *srcs;   /* host array of nsrcs device slices */
@@ -276,14 +288,53 @@ typedef struct fgfc_noalloc_job {
  *
  * The first call on a device looks up the array's device address (once per
  * device, with that device current); make that first call before any stream
- * capture. Every call reuses the same array and leaves its contents behind:
- * calls whose work overlaps on the GPU (different streams, or different
- * threads without ordering) race on it; calls on one stream are ordered.
- * Host threads are serialised by a lock around the call itself. */
+ * capture. A call made while `stream` is being captured returns FGFC_ERR_ARG
+ * and enqueues nothing. Every call reuses the same array and leaves its
+ * contents behind: calls whose work overlaps on the GPU (different streams,
+ * or different threads without ordering) race on it; calls on one stream are
+ * ordered. Host threads are serialised by a lock around the call itself.
+ *
+ * The descriptors are built in a fixed, pageable host array and copied in
+ * with one cudaMemcpyAsync, which CUDA stages before returning: the call may
+ * block the host until `stream` has reached that copy. Stripes are grouped as
+ * in fgfc_batch_run (Gf8 stripes of at most 4 rows and 14 sources on the
+ * byte-table kernel, the rest by their number of 4-byte row groups), one
+ * launch per group. */
 #define FGFC_NOALLOC_SCRATCH_BYTES (8u << 20)
 #define FGFC_NOALLOC_MAX_ROWS_GF8 16
 fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job *jobs, size_t njobs,
                                    fgfc_stream stream);
+
+/* ---------------------------------------------------------------- kernel choice and tuning */
+
+/* No reference counterpart as such: the reference picks its CPU backend once
+ * (src/kernel/mod.rs:147-184) and routes each call between blocked and AXPY
+ * paths by shape (src/kernel/gf16.rs:419-460). Here a matrix call runs one of
+ * three kernel families, chosen per (field, sources, rows, row-length bucket)
+ * by, in order: a process-wide override (fgfc_tune_force, or the environment
+ * variable FGFC_KERNEL = nibble | byte | gf2mma, read once), the table of
+ * measured winners (fgfc_tune_shape; fgfc_tune_save / fgfc_tune_load persist
+ * it as JSON), and built-in rules. A family is only ever used for shapes it
+ * can run; every family gives the same bytes. */
+typedef enum fgfc_kernel {
+  FGFC_KERNEL_AUTO = 0,   /* the tuned or built-in choice */
+  FGFC_KERNEL_NIBBLE = 1, /* split-nibble product tables in shared memory (every shape) */
+  FGFC_KERNEL_BYTE = 2,   /* 256-entry byte tables: Gf8, at most 4 rows and 14 sources */
+  FGFC_KERNEL_GF2MMA = 3  /* bit-sliced GF(2) contraction on the tensor cores (tcgen05) */
+} fgfc_kernel;
+
+fgfc_status fgfc_tune_force(fgfc_kernel kernel);
+/* The family a matrix call of this shape runs now. */
+fgfc_kernel fgfc_tune_choice(fgfc_field field, size_t nsrcs, size_t nrows, size_t row_len);
+/* 1 if `kernel` can run this shape. */
+int fgfc_tune_usable(fgfc_kernel kernel, fgfc_field field, size_t nsrcs, size_t nrows);
+/* Times every usable family on a dot_product_matrix_with call of this shape
+ * on the current device (allocates and frees its own buffers) and records the
+ * fastest for the shape's row-length bucket; the winner goes to *out. */
+fgfc_status fgfc_tune_shape(fgfc_field field, size_t nsrcs, size_t nrows, size_t row_len, fgfc_kernel *out);
+fgfc_status fgfc_tune_save(const char *path);
+fgfc_status fgfc_tune_load(const char *path);
+void fgfc_tune_clear(void);
 
 /* ---------------------------------------------------------------- serving loop */
 
@@ -327,10 +378,10 @@ typedef struct fgfc_request {
   size_t nsrcs;
   uint8_t *dst;             /* host destination */
   size_t dst_len;
-  const size_t *row_starts; /* NULL: rows j * row_len; else scattered rows (accumulate) */
+  const size_t *row_starts; /* NULL: rows j * row_len; else scattered rows */
   size_t nrows;
   size_t row_len;
-  int overwrite;            /* 1: dot_product_matrix; 0: accumulate */
+  int overwrite;            /* 1: dot_product_matrix (scattered: its overwrite extension); 0: accumulate */
 } fgfc_request;
 
 typedef struct fgfc_server_stats {

@@ -1,9 +1,12 @@
-"""fgfc_batch_run_noalloc: the work-list kernel on a fixed device scratch
-array. Each call must give, byte for byte, what the allocating raw entry
-points (fgfc_dot_product_matrix, fgfc_mul_add_matrix,
-fgfc_mul_add_matrix_scattered) give on the same inputs, and two calls in a
-row must not see each other's scratch. Collected last on purpose: it also
-has to pass after everything else has run in the same process."""
+"""fgfc_batch_run_noalloc: the work-list kernels on a fixed device scratch
+array, for callers that may not allocate device memory while they run.
+Each call must give, byte for byte, what the allocating raw entry points
+(fgfc_dot_product_matrix, fgfc_mul_add_matrix,
+fgfc_mul_add_matrix_scattered) give on the same inputs and what the CPU
+oracle gives, two calls in a row must not see each other's scratch, and the
+calls must leave the device's free memory unchanged. Collected last on
+purpose: it also has to pass after everything else has run in the same
+process."""
 import ctypes as C
 
 import numpy as np
@@ -11,12 +14,14 @@ import pytest
 import torch
 
 from fgf_b200 import _lib, ops
-from fgf_b200.fields import Gf8D, Gf16, Gf32
+from fgf_b200.fields import Gf8B, Gf8D, Gf16, Gf32
+from oracle import orc
 
 pytestmark = pytest.mark.gpu
 
 SCRATCH = 8 << 20
 ERR_LIMIT = 12
+ERR_ARG = 11
 MAX_ROWS = {Gf8D: 16, Gf16: 8, Gf32: 4}
 
 
@@ -78,7 +83,26 @@ def _expected(field, stripe):
     return want
 
 
+def _oracle(field, stripe):
+    """The CPU oracle's result for one stripe (host arrays)."""
+    k, m, rl, kind, coeffs, srcs, dst, starts = stripe
+    out = dst.cpu().numpy().copy()
+    hs = [s.cpu().numpy().copy() for s in srcs]
+    if kind == "scatter":
+        orc.mul_add_matrix_scattered(field.ID, out, rl, starts, coeffs, hs)
+    elif kind == "dot":
+        orc.dot_product_matrix(field.ID, out, rl, m, coeffs, hs)
+    else:
+        orc.mul_add_matrix(field.ID, out, rl, m, coeffs, hs)
+    return out
+
+
 CASES = {
+    Gf8B: [
+        (10, 4, 32768 + 16, "dot", 0),      # byte-table class, K = 10
+        (14, 2, 4096 + 3, "scatter", 0),    # byte-table class, K = 14
+        (16, 9, 3000, "add", 0),            # nibble class, 3 groups
+    ],
     Gf8D: [
         (10, 4, 65536 + 5, "dot", 0),      # RS(10,4) encode shape
         (20, 16, 4099, "add", 0),          # most rows, sources processed in chunks
@@ -98,18 +122,55 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("field", [Gf8D, Gf16, Gf32], ids=lambda f: f.__name__)
+@pytest.mark.parametrize("field", [Gf8B, Gf8D, Gf16, Gf32], ids=lambda f: f.__name__)
 def test_two_calls_in_a_row_match_the_allocating_entry_points(cuda, field):
     for call, seed in enumerate((11, 12)):
         stripes = _stripes(field, CASES[field], seed + 100 * field.ID)
         want = [_expected(field, s) for s in stripes]
+        truth = [_oracle(field, s) for s in stripes]
         keep = []
         jobs = [_job(field, s[4], s[5], s[6], s[2], s[1], s[3] == "dot", s[7], keep) for s in stripes]
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         st = _run(field, jobs, torch.cuda.current_stream().cuda_stream)
         assert st == 0, _lib.lib().fgfc_last_error().decode()
         torch.cuda.synchronize()
-        for i, (s, w) in enumerate(zip(stripes, want)):
+        if call:  # the first call may load its kernels' code onto the device
+            assert torch.cuda.mem_get_info()[0] == free_before, "the call changed the device's free memory"
+        for i, (s, w, o) in enumerate(zip(stripes, want, truth)):
             assert torch.equal(s[6], w), f"call {call}, stripe {i} ({s[3]}, k={s[0]}, m={s[1]}) differs"
+            assert np.array_equal(s[6].cpu().numpy(), o), f"call {call}, stripe {i} differs from the oracle"
+
+
+def test_free_memory_unchanged_over_repeated_calls(cuda):
+    stripes = _stripes(Gf8D, CASES[Gf8D], 21)
+    keep = []
+    jobs = [_job(Gf8D, s[4], s[5], s[6], s[2], s[1], s[3] == "dot", s[7], keep) for s in stripes]
+    stream = torch.cuda.current_stream().cuda_stream
+    assert _run(Gf8D, jobs, stream) == 0  # first call on this device: address lookup
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert _run(Gf8D, jobs, stream) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+
+def test_a_capturing_stream_is_refused(cuda):
+    stripes = _stripes(Gf8D, [(4, 2, 4096, "dot", 0)], 22)
+    keep = []
+    s = stripes[0]
+    job = _job(Gf8D, s[4], s[5], s[6], s[2], s[1], True, None, keep)
+    before = s[6].clone()
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        st = _run(Gf8D, [job], side.cuda_stream)
+    assert st == ERR_ARG
+    assert "captured" in _lib.lib().fgfc_last_error().decode()
+    torch.cuda.synchronize()
+    assert torch.equal(s[6], before)
 
 
 def test_empty_and_zero_source_jobs(cuda):
