@@ -95,6 +95,25 @@ class Request(C.Structure):
     ]
 
 
+class RebuildRequest(C.Structure):
+    """`fgfc_rebuild_request`: a reconstruct by erasure pattern."""
+
+    _fields_ = [
+        ("field", C.c_int),
+        ("parity", C.POINTER(c_u32)),
+        ("k", c_size),
+        ("m", c_size),
+        ("survivors", C.POINTER(c_size)),
+        ("srcs", C.POINTER(Slice)),
+        ("erased", C.POINTER(c_size)),
+        ("nerased", c_size),
+        ("dst", C.c_void_p),
+        ("dst_len", c_size),
+        ("row_starts", C.POINTER(c_size)),
+        ("row_len", c_size),
+    ]
+
+
 class ServerStats(C.Structure):
     """`fgfc_server_stats`."""
 
@@ -161,6 +180,11 @@ _SIGS = {
                                                       C.c_void_p, C.POINTER(Slice), c_size, c_stream]),
     "fgfc_dot_product_matrix_scattered_with": (c_status, [c_u8p, c_size, c_size, C.POINTER(c_size), c_size,
                                                           C.c_void_p, C.POINTER(Slice), c_size, c_stream]),
+    "fgfc_cauchy_matrix": (c_status, [C.c_int, c_size, c_size, c_u32, C.POINTER(c_u32)]),
+    "fgfc_decode_matrix": (c_status, [C.c_int, C.POINTER(c_u32), c_size, c_size, C.POINTER(c_size),
+                                      C.POINTER(c_size), c_size, C.POINTER(c_u32)]),
+    "fgfc_decode_plan_create": (c_status, [C.c_int, C.POINTER(c_u32), c_size, c_size, C.POINTER(c_size),
+                                           C.POINTER(c_size), c_size, C.POINTER(C.c_void_p)]),
     "fgfc_batch_create": (c_status, [C.POINTER(C.c_void_p)]),
     "fgfc_batch_destroy": (None, [C.c_void_p]),
     "fgfc_batch_set_graphs": (c_status, [C.c_void_p, C.c_int]),
@@ -168,6 +192,7 @@ _SIGS = {
     "fgfc_batch_stats": (c_status, [C.c_void_p, C.POINTER(c_size), C.POINTER(c_size), C.POINTER(C.c_int)]),
     "fgfc_batch_run_noalloc": (c_status, [C.c_int, C.POINTER(NoAllocJob), c_size, c_stream]),
     "fgfc_run_jobs_serial": (c_status, [C.POINTER(MatrixJob), c_size, c_stream]),
+    "fgfc_device_check": (c_status, [C.c_int]),
     "fgfc_tune_force": (c_status, [C.c_int]),
     "fgfc_tune_choice": (C.c_int, [C.c_int, c_size, c_size, c_size]),
     "fgfc_tune_usable": (C.c_int, [C.c_int, C.c_int, c_size, c_size]),
@@ -177,6 +202,7 @@ _SIGS = {
     "fgfc_tune_clear": (None, []),
     "fgfc_server_create": (c_status, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
     "fgfc_server_submit": (c_status, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "fgfc_server_submit_rebuild": (c_status, [C.c_void_p, C.POINTER(RebuildRequest), C.POINTER(C.c_uint64)]),
     "fgfc_server_wait": (c_status, [C.c_void_p, C.c_uint64]),
     "fgfc_server_poll": (c_status, [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]),
     "fgfc_server_drain": (c_status, [C.c_void_p]),

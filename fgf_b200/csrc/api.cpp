@@ -80,6 +80,10 @@ struct fgfc_plan {
   int field;
   size_t rows, cols;
   std::vector<uint32_t> values;
+  // GF(2) bit matrices for the tensor-core kernel, per orientation (matrix:
+  // rows x cols; scatter: 1 x len; gather: len x 1), empty where the shape
+  // is outside that kernel's range
+  std::vector<uint32_t> bits_mat, bits_scat, bits_gath;
   int device;
   uint32_t* dev;        // device tables, three orientations back to back
   size_t mat_groups;    // groups per source in the matrix orientation
@@ -95,14 +99,72 @@ struct CoeffSrc {
   const uint32_t* host = nullptr;  // term-major k x m
   const uint32_t* dev = nullptr;   // compact tables [(t*E+p)*gstride + g][32]
   size_t gstride = 0;
+  const uint32_t* bits = nullptr;  // GF(2) bit matrix (plans), or built from `host` when needed
 };
 
 std::mutex g_launch_mu;
 
 fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows,
                        size_t m, const CoeffSrc& cs, size_t len, bool overwrite,
-                       cudaStream_t stream, const char* name) {
+                       cudaStream_t stream, const char* name, bool allow_mma = true);
+
+// The tensor-core contraction for the 16-byte-aligned body of a call whose
+// sources and rows all share one offset within 16 bytes; the columns before
+// and after the body go to the table kernels. Returns false (nothing
+// enqueued) when the call does not qualify.
+bool run_gf2mma(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
+                const CoeffSrc& cs, size_t len, bool overwrite, cudaStream_t stream, const char* name,
+                fgfc_status* st) {
+  const int E = field_bytes(field);
+  const uintptr_t al = reinterpret_cast<uintptr_t>(srcs[0]) & 15;
+  if (al % E) return false;
+  for (size_t t = 0; t < k; ++t)
+    if ((reinterpret_cast<uintptr_t>(srcs[t]) & 15) != al) return false;
+  for (size_t j = 0; j < m; ++j)
+    if ((reinterpret_cast<uintptr_t>(rows[j]) & 15) != al) return false;
+  const size_t head = std::min<size_t>((16 - al) & 15, len);
+  const size_t blk_bytes = 512 * static_cast<size_t>(E);
+  const uint64_t nblk = (len - head) / blk_bytes;
+  if (!nblk) return false;
+  std::vector<uint32_t> tmp;
+  const uint32_t* bits = cs.bits;
+  if (!bits) {
+    tmp.resize(kGf2BitWords);
+    gf2mma_bits(field, cs.host, k, m, tmp.data());
+    bits = tmp.data();
+  }
+  std::vector<const uint8_t*> sp(k);
+  std::vector<uint8_t*> rp(m);
+  for (size_t t = 0; t < k; ++t) sp[t] = srcs[t] + head;
+  for (size_t j = 0; j < m; ++j) rp[j] = rows[j] + head;
+  cudaError_t e = gf2mma_launch(field, sp.data(), k, rp.data(), m, bits, nblk, overwrite, stream);
+  if (e != cudaSuccess) {
+    *st = cuda_fail(e, name);
+    return true;
+  }
+  const size_t body_end = head + nblk * blk_bytes;
+  if (head) {
+    *st = run_matrix(field, srcs, k, rows, m, cs, head, overwrite, stream, name, false);
+    if (*st != FGFC_OK) return true;
+  }
+  if (body_end < len) {
+    for (size_t t = 0; t < k; ++t) sp[t] = srcs[t] + body_end;
+    for (size_t j = 0; j < m; ++j) rp[j] = rows[j] + body_end;
+    *st = run_matrix(field, sp.data(), k, rp.data(), m, cs, len - body_end, overwrite, stream, name, false);
+    if (*st != FGFC_OK) return true;
+  }
+  *st = ok();
+  return true;
+}
+
+fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows,
+                       size_t m, const CoeffSrc& cs, size_t len, bool overwrite,
+                       cudaStream_t stream, const char* name, bool allow_mma) {
   if (m == 0 || len == 0) return ok();
+  if (allow_mma && k > 0 && (cs.bits || cs.host) && choose_kernel(field, k, m, len) == FGFC_KERNEL_GF2MMA) {
+    fgfc_status st;
+    if (run_gf2mma(field, srcs, k, rows, m, cs, len, overwrite, stream, name, &st)) return st;
+  }
   if (k == 0) {
     if (overwrite) {
       cudaError_t e = launch_zero_rows(rows, static_cast<int>(m), len, stream);
@@ -202,6 +264,18 @@ fgfc_status upload_plan_tables(fgfc_plan* p) {
     // gather orientation: source i has the single coefficient values[i]
     build_compact_tables(p->field, p->values.data(), 1, 0, len, 0, 1, host.data() + p->off_gath);
   }
+  if (n_mat && gf2mma_shape_ok(p->field, p->rows, p->cols)) {
+    p->bits_mat.resize(kGf2BitWords);
+    gf2mma_bits(p->field, p->values.data(), p->rows, p->cols, p->bits_mat.data());
+  }
+  if (len && gf2mma_shape_ok(p->field, 1, len)) {
+    p->bits_scat.resize(kGf2BitWords);
+    gf2mma_bits(p->field, p->values.data(), 1, len, p->bits_scat.data());
+  }
+  if (len && gf2mma_shape_ok(p->field, len, 1)) {
+    p->bits_gath.resize(kGf2BitWords);
+    gf2mma_bits(p->field, p->values.data(), len, 1, p->bits_gath.data());
+  }
   cudaError_t e = cudaGetDevice(&p->device);
   if (e != cudaSuccess) return cuda_fail(e, "Plan::matrix");
   e = cudaMalloc(&p->dev, host.size() * sizeof(uint32_t));
@@ -216,18 +290,21 @@ CoeffSrc plan_mat(const fgfc_plan* p) {
   CoeffSrc c;
   c.dev = p->dev + p->off_mat;
   c.gstride = p->mat_groups;
+  c.bits = p->bits_mat.empty() ? nullptr : p->bits_mat.data();
   return c;
 }
 CoeffSrc plan_scat(const fgfc_plan* p) {
   CoeffSrc c;
   c.dev = p->dev + p->off_scat;
   c.gstride = p->scat_groups;
+  c.bits = p->bits_scat.empty() ? nullptr : p->bits_scat.data();
   return c;
 }
 CoeffSrc plan_gath(const fgfc_plan* p) {
   CoeffSrc c;
   c.dev = p->dev + p->off_gath;
   c.gstride = 1;
+  c.bits = p->bits_gath.empty() ? nullptr : p->bits_gath.data();
   return c;
 }
 
@@ -236,6 +313,13 @@ CoeffSrc plan_gath(const fgfc_plan* p) {
 extern "C" {
 
 const char* fgfc_last_error(void) { return t_err.c_str(); }
+
+fgfc_status fgfc_device_check(int clear) {
+  const int w = gf2mma_error(clear != 0);
+  if (w < 0) return fail(FGFC_ERR_CUDA, "device_check: cannot read the device error word");
+  if (w) return fail(FGFC_ERR_CUDA, "device_check: a tensor-core kernel gave up waiting (code %d)", w);
+  return ok();
+}
 const char* fgfc_version(void) { return "fgf-cuda 0.1.0 (sm_100a; mirrors fgf 0.4.0 ops)"; }
 
 void fgfc_limits(size_t* max_sources, size_t* max_rows) {

@@ -1,11 +1,604 @@
-// gf2mma.cu -- bit-sliced GF(2) contraction of the matrix ops on the tensor
-// cores (tcgen05). Shapes it covers are reported by gf2mma_shape_ok.
+// gf2mma.cu -- the matrix ops as a bit-sliced GF(2) contraction on the
+// tensor cores (tcgen05, sm_100a).
+//
+// Multiplying a packed element by a fixed coefficient is linear over GF(2):
+// the 8E output bits of c * x are XORs of the 8E input bits of x. So for one
+// element column (one element position of every source and row) the whole
+// op rows[j] (^)= XOR_t c[t][j] * src_t is one GF(2) matrix-vector product:
+// out (8E * m bits) = B (8E*m x 8E*k) . in (8E*k bits). It is evaluated as an
+// integer matrix product whose low bit is the parity:
+//
+//   D[col][n] = sum_kappa A[col][kappa] * B[kappa][n]     (tcgen05.mma kind::i8)
+//
+// with A the input bits of 128 element columns (M = 128, one TMEM lane per
+// column) and B the plan's bit matrix (N = output bits, K = input bits). The
+// input bit b of a byte enters A as the value 2^b (the byte masked with
+// 0x01010101 << b, one LOP3 per 4 values) and B holds 2^(7-b) where the bit
+// matrix has a 1, so every product is 0 or 128 and D = 128 * (number of 1
+// products): its bit 7 is the GF(2) sum, bits 0..6 are zero. Sums stay below
+// 2^23 (at most 512 products of 2^14), so the int32 accumulator is exact.
+//
+// Layout and flow of one CTA (one per SM, persistent over 512-column blocks):
+//   * warp 4 (producer): stages the k source rows of a block (512 columns,
+//     512 * E bytes per source) into a 4-deep shared-memory ring with
+//     cp.async.bulk (single GPU, no multicast), completion on an mbarrier;
+//   * warps 0..3 (workers, thread i owns TMEM lane i): read the 4 consecutive
+//     columns 4i..4i+3 of every source of a block into registers, then for
+//     each of the block's 4 tiles (tile q = columns 4i + q) build the A lane
+//     (K/4 32-bit TMEM columns) and write it with tcgen05.st; after a tile's
+//     product is done they read D back (tcgen05.ld), gather bit 7 of every
+//     accumulator into output bytes with PRMT and two multiply-adds, and
+//     after the 4th tile store 4 consecutive columns of every row;
+//   * warp 5 (issuer): allocates TMEM (A and D double-buffered, 512 columns),
+//     issues K/32 tcgen05.mma per tile from one thread and commits each tile
+//     to an mbarrier.
+// Every mbarrier wait is bounded: a wait that runs out sets the error word,
+// stops the CTA's loops, waits (bounded) for its own copies and products in
+// flight and frees TMEM before returning.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "fast_core.cuh"
 #include "internal.hpp"
 
 namespace fgfc {
 
-bool gf2mma_shape_ok(int, size_t, size_t) { return false; }
+namespace {
+
+constexpr int kMmaThreads = 192;       // 4 worker warps, producer, issuer
+constexpr int kStages = 4;
+constexpr uint32_t kCols = 512;        // element columns per block (4 tiles of 128)
+constexpr uint32_t kMaxInBits = 512;   // K
+constexpr uint32_t kMaxOutBits = 128;  // N
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+struct Gf2Launch {
+  const uint8_t* src[kMaxSrc];  // kMaxSrc >= 64 sources
+  uint8_t* dst[16];             // rows
+  uint64_t nblk;                // 512-column blocks
+  uint32_t k, m, E;
+  uint32_t ngroups;             // K / 32: groups of 4 input bytes
+  uint32_t npad;                // N: output bits padded to a multiple of 16
+  uint32_t overwrite;
+  int* err;                     // device error word (0 = fine)
+  // bits[n][g]: bit (8r + b) set iff output bit n takes input byte 4g + r, bit b
+  uint32_t bits[kMaxOutBits][kMaxInBits / 32];
+};
+static_assert(sizeof(Gf2Launch) <= 32000, "launch parameter block too large");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait; false when it ran out. With `honor_abort` it also gives up
+// once another role has aborted (the drain waits before exit do not).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, bool honor_abort = true) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try(b, parity)) return true;
+    if (honor_abort && (i & 1023u) == 1023u && *abort) return false;
+  }
+  return false;
+}
+
+// The same wait by every lane of a warp, with a warp-uniform result (the
+// tcgen05 .sync.aligned instructions that follow need the whole warp).
+__device__ __forceinline__ bool warp_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
+  const bool ok = mbar_wait(b, parity, abort);
+  return __all_sync(0xffffffffu, ok);
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+        "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr)
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
+// rows x 16 bytes (128 contiguous bytes); `lbo` = bytes between the two
+// 16-byte K halves of a 32-byte K step, `sbo` = bytes between 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Output byte from 8 accumulators (bit o of the byte = bit 7 of r[o]).
+__device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
+  const uint32_t p03 = prmt(prmt(r[0], r[1], 0x0040u), prmt(r[2], r[3], 0x0040u), 0x5410u);
+  const uint32_t p47 = prmt(prmt(r[4], r[5], 0x0040u), prmt(r[6], r[7], 0x0040u), 0x5410u);
+  // bit 7 of byte i of p03 -> bit 24 + i; of p47 -> bit 28 + i (no carries:
+  // every shifted copy lands on a distinct bit)
+  return (p03 >> 4) * 0x00204081u + p47 * 0x00204081u;  // output byte in bits 24..31
+}
+
+struct Smem {
+  uint64_t full[kStages], empty[kStages], afull[2], dfull[2];
+  uint32_t tmem_base;
+  int abort;
+};
+
+// Epilogue of tile tt (columns 4i + q of its block, q = tt % 4, TMEM buffer
+// tt % 2): read the accumulators, fold bit 7 of each into output byte v of
+// column q (byte q of out[v]); after the 4th tile store 4 columns of every row.
+template <int E, int Q>
+__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
+                                         uint32_t (&out)[16], volatile int* abort) {
+  constexpr uint32_t b = Q & 1;
+  constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
+  const uint32_t warp = threadIdx.x >> 5, i = threadIdx.x;
+  const uint32_t lane_base = (warp * 32u) << 16;
+  if (!warp_wait(&S.dfull[b], static_cast<uint32_t>((tt >> 1) & 1u), abort)) return false;
+  tc_fence_after();
+  const uint32_t nout = a.m * E;
+#pragma unroll
+  for (uint32_t c = 0; c < kMaxOutBits / 32; ++c) {
+    const uint32_t c0 = 32u * c;
+    if (c0 >= a.npad) break;
+    uint32_t r[32];
+    if (a.npad - c0 >= 32) {
+      tmem_ld32(lane_base | (d_col[b] + c0), r);
+    } else {
+      tmem_ld16(lane_base | (d_col[b] + c0), r);
+#pragma unroll
+      for (int x = 16; x < 32; ++x) r[x] = 0;
+    }
+    tmem_wait_ld();
+#pragma unroll
+    for (uint32_t v = 0; v < 4; ++v)
+      if (4 * c + v < nout) out[4 * c + v] = prmt(out[4 * c + v], pack_byte(&r[8 * v]), qsel);
+  }
+  if (Q == 3) {
+    const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
+    const uint64_t off = blk * kCols * E + static_cast<uint64_t>(i) * 4u * E;
+#pragma unroll
+    for (uint32_t j = 0; j < 16 / E; ++j) {
+      if (j >= a.m) break;
+      uint8_t* p = a.dst[j] + off;
+      if (E == 1) {
+        uint32_t v = out[j];
+        if (!a.overwrite) v ^= *reinterpret_cast<const uint32_t*>(p);
+        *reinterpret_cast<uint32_t*>(p) = v;
+      } else if (E == 2) {
+        uint2 v = make_uint2(prmt(out[2 * j], out[2 * j + 1], 0x5140u), prmt(out[2 * j], out[2 * j + 1], 0x7362u));
+        if (!a.overwrite) {
+          const uint2 d = *reinterpret_cast<const uint2*>(p);
+          v.x ^= d.x;
+          v.y ^= d.y;
+        }
+        *reinterpret_cast<uint2*>(p) = v;
+      } else {
+        uint4 v = make_uint4(row_word4(&out[4 * j], 0), row_word4(&out[4 * j], 1), row_word4(&out[4 * j], 2),
+                             row_word4(&out[4 * j], 3));
+        if (!a.overwrite) {
+          const uint4 d = *reinterpret_cast<const uint4*>(p);
+          v.x ^= d.x;
+          v.y ^= d.y;
+          v.z ^= d.z;
+          v.w ^= d.w;
+        }
+        *reinterpret_cast<uint4*>(p) = v;
+      }
+    }
+  }
+  return true;
+}
+
+// The A lane of tile Q (column 4i + Q of the block) into TMEM buffer Q % 2.
+// Group g = input bytes 4g..4g+3 of the column (input byte u = t * E + p);
+// TMEM column 8g + b holds bit b of those 4 bytes, each as the value 2^b.
+template <int E, int Q>
+__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[64], uint32_t a_col) {
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t lane_base = (warp * 32u) << 16;
+  const uint32_t nwords = a.k * E;
+#pragma unroll
+  for (uint32_t g0 = 0; g0 < 16; g0 += 4) {
+    if (g0 >= a.ngroups) break;
+    uint32_t col[32];
+#pragma unroll
+    for (uint32_t gg = 0; gg < 4; ++gg) {
+      const uint32_t g = g0 + gg;
+      uint32_t wg;
+      if (E == 1) {  // sources 4g..4g+3, byte Q of each
+        constexpr uint32_t qs = Q | ((4u + Q) << 4);
+        const uint32_t s0 = 4 * g < nwords ? sw[4 * g] : 0u;
+        const uint32_t s1 = 4 * g + 1 < nwords ? sw[4 * g + 1] : 0u;
+        const uint32_t s2 = 4 * g + 2 < nwords ? sw[4 * g + 2] : 0u;
+        const uint32_t s3 = 4 * g + 3 < nwords ? sw[4 * g + 3] : 0u;
+        wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
+      } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
+        const uint32_t x0 = 4 * g + Q / 2 < nwords ? sw[4 * g + Q / 2] : 0u;
+        const uint32_t x1 = 4 * g + 2 + Q / 2 < nwords ? sw[4 * g + 2 + Q / 2] : 0u;
+        wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
+      } else {  // source g, element Q
+        wg = 4 * g + Q < nwords ? sw[4 * g + Q] : 0u;
+      }
+#pragma unroll
+      for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
+    }
+    const uint32_t taddr = lane_base | (a_col + 8u * g0);
+    if (a.ngroups - g0 >= 4) {
+      tmem_st32(taddr, col);
+    } else {
+#pragma unroll
+      for (uint32_t gg = 0; gg < 3; ++gg)
+        if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
+    }
+  }
+  tmem_wait_st();
+}
+
+template <int E>
+__device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
+                                            uint64_t nmine, const uint32_t (&a_col)[2], const uint32_t (&d_col)[2],
+                                            volatile int* abort) {
+  const uint32_t lane = threadIdx.x & 31u, i = threadIdx.x;
+  uint32_t sw[64];   // this thread's 4 columns of every source (k * E words)
+  uint32_t out[16];  // output byte v of the 4 columns
+#pragma unroll
+  for (int x = 0; x < 16; ++x) out[x] = 0;
+  const uint32_t nwords = a.k * E;
+  bool ok = true;
+  uint64_t t = 0;  // tiles expanded so far
+  for (uint64_t it = 0; it < nmine && ok; ++it) {
+    const uint32_t s = static_cast<uint32_t>(it % kStages);
+    if (!warp_wait(&S.full[s], static_cast<uint32_t>((it / kStages) & 1u), abort)) {
+      ok = false;
+      break;
+    }
+    const uint8_t* st = stages + s * stage_bytes;
+#pragma unroll
+    for (uint32_t w = 0; w < 64; w += E) {
+      if (w >= nwords) break;
+      const uint8_t* p = st + (w / E) * kCols * E + i * 4u * E;
+      if (E == 1) {
+        sw[w] = *reinterpret_cast<const uint32_t*>(p);
+      } else if (E == 2) {
+        const uint2 v = *reinterpret_cast<const uint2*>(p);
+        sw[w] = v.x;
+        sw[w + 1] = v.y;
+      } else {
+        const uint4 v = *reinterpret_cast<const uint4*>(p);
+        sw[w] = v.x;
+        sw[w + 1] = v.y;
+        sw[w + 2] = v.z;
+        sw[w + 3] = v.w;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.empty[s]);  // the stage may be refilled
+    // tile Q of this block is tile t + Q; before it reuses buffer Q % 2, the
+    // tile two before it (t + Q - 2) is read back
+#define FGFC_TILE(Q, PQ)                                                      \
+    if (ok && t + Q >= 2) ok = epilogue<E, PQ>(a, S, d_col, t + Q - 2, out, abort); \
+    if (ok) {                                                                 \
+      expand<E, Q>(a, sw, a_col[Q & 1]);                                      \
+      tc_fence_before();                                                      \
+      __syncwarp();                                                           \
+      if (lane == 0) mbar_arrive(&S.afull[Q & 1]);                            \
+    }
+    FGFC_TILE(0, 2)
+    FGFC_TILE(1, 3)
+    FGFC_TILE(2, 0)
+    FGFC_TILE(3, 1)
+#undef FGFC_TILE
+    t += 4;
+  }
+  // the last two tiles (columns 2 and 3 of the last block)
+  if (ok && t >= 2) ok = epilogue<E, 2>(a, S, d_col, t - 2, out, abort);
+  if (ok && t >= 2) ok = epilogue<E, 3>(a, S, d_col, t - 1, out, abort);
+  if (!ok) {
+    atomicExch(a.err, 3);
+    *abort = 1;
+  }
+  (void)nwords;
+}
+
+template <int E>
+__global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_constant__ Gf2Launch a) {
+  // dynamic shared memory: [B image (npad x K bytes)] [stages] [Smem]
+  const uint32_t K = a.ngroups * 32u;
+  const uint32_t b_bytes = (a.npad * K + 1023u) & ~1023u;
+  const uint32_t stage_bytes = (a.k * kCols * E + 127u) & ~127u;
+  uint8_t* bimg = g_smem;
+  uint8_t* stages = g_smem + b_bytes;
+  Smem& S = *reinterpret_cast<Smem*>(stages + kStages * stage_bytes);
+  volatile int* abort = &S.abort;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+
+  // ---- B image: entry (n, kappa = 32 g + 4 b + r) = 2^(7 - b) where output
+  // bit n takes bit b of input byte 4 g + r; core matrix (kappa / 16, n / 8) at
+  // ((kappa / 16) * (npad / 8) + n / 8) * 128, row n % 8, byte kappa % 16
+  for (uint32_t i = threadIdx.x; i < a.npad * K / 16u; i += blockDim.x) {
+    const uint32_t core = i >> 3, row = i & 7u;
+    const uint32_t kc = core / (a.npad / 8u), n = (core % (a.npad / 8u)) * 8u + row;
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      uint32_t v = 0;
+#pragma unroll
+      for (int x = 0; x < 4; ++x) {
+        const uint32_t kappa = kc * 16u + q * 4u + x;
+        const uint32_t g = kappa >> 5, b = (kappa >> 2) & 7u, r = kappa & 3u;
+        const uint32_t bit = (n < kMaxOutBits && g < kMaxInBits / 32u) ? (a.bits[n][g] >> (8u * r + b)) & 1u : 0u;
+        v |= (bit << (7u - b)) << (8 * x);
+      }
+      w[q] = v;
+    }
+    *reinterpret_cast<uint4*>(bimg + static_cast<size_t>(i) * 16u) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], 4);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&S.afull[b], 4);
+      mbar_init(&S.dfull[b], 1);
+    }
+    S.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // generic-proxy writes of the B image become visible to the tensor cores
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = S.tmem_base;
+  const uint32_t a_col[2] = {tbase, tbase + 128u};
+  const uint32_t d_col[2] = {tbase + 256u, tbase + 384u};
+
+  // blocks of this CTA: blockIdx.x, + gridDim.x, ...
+  const uint64_t nmine = a.nblk > blockIdx.x ? (a.nblk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+  const uint64_t ntiles = nmine * 4u;
+
+  if (warp == 4) {
+    // ---- producer
+    uint64_t issued = 0;
+    if (lane == 0) {
+      const uint32_t row_bytes = kCols * E;
+      for (uint64_t i = 0; i < nmine && !*abort; ++i) {
+        const uint32_t s = static_cast<uint32_t>(i % kStages);
+        if (i >= kStages && !mbar_wait(&S.empty[s], static_cast<uint32_t>((i / kStages - 1) & 1u), abort)) {
+          atomicExch(a.err, 1);
+          *abort = 1;
+          break;
+        }
+        const uint64_t blk = blockIdx.x + i * gridDim.x;
+        mbar_expect_tx(&S.full[s], a.k * row_bytes);
+        for (uint32_t t = 0; t < a.k; ++t)
+          bulk_g2s(stages + s * stage_bytes + t * row_bytes, a.src[t] + blk * row_bytes, row_bytes, &S.full[s]);
+        ++issued;
+      }
+      // copies still in flight must land before the CTA exits
+      for (uint64_t i = issued > kStages ? issued - kStages : 0; i < issued; ++i)
+        mbar_wait(&S.full[i % kStages], static_cast<uint32_t>((i / kStages) & 1u), abort, false);
+    }
+  } else if (warp == 5) {
+    // ---- issuer: one thread issues every product of a tile
+    if (lane == 0) {
+      const uint32_t idesc = (2u << 4) | ((a.npad >> 3) << 17) | ((128u >> 4) << 24);  // s32 += u8 * u8, M = 128
+      const uint32_t bsm = smem_u32(bimg);
+      const uint32_t lbo = a.npad * 16u, sbo = 128u;
+      uint64_t t = 0;
+      for (; t < ntiles && !*abort; ++t) {
+        const uint32_t b = static_cast<uint32_t>(t & 1u);
+        if (!mbar_wait(&S.afull[b], static_cast<uint32_t>((t >> 1) & 1u), abort)) {
+          atomicExch(a.err, 2);
+          *abort = 1;
+          break;
+        }
+        tc_fence_after();
+        for (uint32_t g = 0; g < a.ngroups; ++g)
+          mma_i8(d_col[b], a_col[b] + 8u * g, smem_desc(bsm + g * 2u * a.npad * 16u, lbo, sbo), idesc, g > 0);
+        mma_commit(&S.dfull[b]);
+      }
+      // the last products must finish before TMEM is freed
+      for (uint64_t u = t > 2 ? t - 2 : 0; u < t; ++u)
+        mbar_wait(&S.dfull[u & 1u], static_cast<uint32_t>((u >> 1) & 1u), abort, false);
+    }
+  } else {
+    // ---- workers: thread i owns TMEM lane i and columns 4i..4i+3 of a block
+    worker_loop<E>(a, S, stages, stage_bytes, nmine, a_col, d_col, abort);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 5)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+}
+
+// Per-device error word for the kernel's bounded waits.
+int* error_word() {
+  static std::mutex mu;
+  static int* words[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!words[dev]) {
+    int* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+    cudaMemset(p, 0, sizeof(int));
+    words[dev] = p;
+  }
+  return words[dev];
+}
+
+}  // namespace
+
+bool gf2mma_shape_ok(int field, size_t k, size_t m) {
+  const int E = field_bytes(field);
+  return E > 0 && k >= 1 && m >= 1 && k * E <= kMaxInBits / 8 && m * E <= kMaxOutBits / 8;
+}
+
+// Bit matrix of a coefficient matrix (term-major, k x m): bits[n][g] bit
+// (8r + b) = output bit n (byte n / 8 of the m*E output bytes, bit n % 8)
+// depends on bit b of input byte 4g + r (input byte u = t * E + p).
+void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t* bits /* [128][16] */) {
+  const int E = field_bytes(field);
+  std::memset(bits, 0, kMaxOutBits * (kMaxInBits / 32) * sizeof(uint32_t));
+  for (size_t t = 0; t < k; ++t)
+    for (size_t j = 0; j < m; ++j) {
+      uint8_t M[4][4];
+      coeff_byte_matrix(field, coeffs[t * m + j] & field_mask(field), M);
+      for (int o = 0; o < E; ++o)
+        for (int p = 0; p < E; ++p) {
+          if (!M[o][p]) continue;
+          const size_t u = t * E + p;
+          for (int b = 0; b < 8; ++b) {
+            const uint8_t prod = byte_mul(field, M[o][p], static_cast<uint8_t>(1u << b));
+            for (int ob = 0; ob < 8; ++ob)
+              if ((prod >> ob) & 1u) {
+                const size_t n = (j * E + o) * 8 + ob;
+                bits[n * (kMaxInBits / 32) + u / 4] |= 1u << (8 * (u % 4) + b);
+              }
+          }
+        }
+    }
+}
+
+// Rows [0, nblk * 512 * E) of every source and row, all 16-byte aligned.
+cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
+                          const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream) {
+  if (!nblk) return cudaSuccess;
+  const int E = field_bytes(field);
+  static thread_local Gf2Launch a;
+  for (size_t t = 0; t < k; ++t) a.src[t] = srcs[t];
+  for (size_t j = 0; j < m; ++j) a.dst[j] = rows[j];
+  a.nblk = nblk;
+  a.k = static_cast<uint32_t>(k);
+  a.m = static_cast<uint32_t>(m);
+  a.E = static_cast<uint32_t>(E);
+  a.ngroups = static_cast<uint32_t>((k * E + 3) / 4);
+  a.npad = static_cast<uint32_t>((m * E * 8 + 15) / 16 * 16);
+  a.overwrite = overwrite ? 1u : 0u;
+  a.err = error_word();
+  if (!a.err) return cudaErrorMemoryAllocation;
+  std::memcpy(a.bits, bits, sizeof a.bits);
+  const uint32_t K = a.ngroups * 32u;
+  const uint32_t b_bytes = (a.npad * K + 1023u) & ~1023u;
+  const uint32_t stage_bytes = (a.k * kCols * E + 127u) & ~127u;
+  const int smem = static_cast<int>(b_bytes + kStages * stage_bytes + sizeof(Smem));
+  const void* fn = E == 1 ? reinterpret_cast<const void*>(gf2mma_kernel<1>)
+                          : (E == 2 ? reinterpret_cast<const void*>(gf2mma_kernel<2>)
+                                    : reinterpret_cast<const void*>(gf2mma_kernel<4>));
+  // one CTA per SM: TMEM (512 columns) is allocated whole
+  const int smem_launch = std::max(smem, 116 * 1024);
+  cudaError_t e = ensure_smem_attr(fn, smem_launch);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(nblk, static_cast<uint64_t>(sm_count())));
+  if (E == 1)
+    gf2mma_kernel<1><<<grid, kMmaThreads, smem_launch, stream>>>(a);
+  else if (E == 2)
+    gf2mma_kernel<2><<<grid, kMmaThreads, smem_launch, stream>>>(a);
+  else
+    gf2mma_kernel<4><<<grid, kMmaThreads, smem_launch, stream>>>(a);
+  return cudaGetLastError();
+}
+
+// Error word of the current device: nonzero when a bounded wait ran out.
+int gf2mma_error(bool clear) {
+  int* p = error_word();
+  if (!p) return -1;
+  int v = 0;
+  if (cudaMemcpy(&v, p, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (clear && v) cudaMemset(p, 0, sizeof(int));
+  return v;
+}
 
 }  // namespace fgfc

@@ -74,6 +74,16 @@ int choose_kernel(int field, size_t k, size_t m, size_t len);
 // Shapes the bit-sliced tensor-core contraction covers in one launch
 // (gf2mma.cu): at most 512 input bits and 128 output bits per element column.
 bool gf2mma_shape_ok(int field, size_t k, size_t m);
+// Compact GF(2) bit matrix of a term-major k x m coefficient matrix:
+// kGf2BitWords words, [output bit][input word group].
+constexpr size_t kGf2BitWords = 128 * 16;
+void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t* bits);
+// Columns [0, nblk * 512 * E) of k sources and m rows, all 16-byte aligned.
+cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
+                          const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream);
+// Error word of the current device's tensor-core kernels (0 = fine);
+// synchronises with the device.
+int gf2mma_error(bool clear);
 // Opt `fn` in to `bytes` of dynamic shared memory on the current device, once
 // per (device, kernel); thread-safe.
 cudaError_t ensure_smem_attr(const void* fn, int bytes);
@@ -110,6 +120,11 @@ const char* last_error_text();
 fgfc_status validate_matrix_call(int field, const char* name, size_t dst_len, size_t row_len,
                                  const size_t* row_starts, size_t nrows, const fgfc_slice* srcs, size_t nsrcs,
                                  const uint32_t* coeffs, int overwrite);
+
+// Decode rows of the code [I_k ; parity] for a survivor set and erased shards,
+// term-major k x nerased (decode.cpp).
+fgfc_status decode_matrix(int field, const uint32_t* parity, size_t k, size_t m, const size_t* survivors,
+                          const size_t* erased, size_t nerased, uint32_t* out);
 
 // fgfc_batch_run_noalloc's work (batch.cu): jobs already validated against
 // the ops' rules; returns 0 or an fgfc_status with `msg` set.

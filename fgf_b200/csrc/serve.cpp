@@ -98,6 +98,78 @@ class Arena {
   size_t size_ = 0, used_ = 0;
 };
 
+// Page-locked staging copies split over a few host threads: one thread's
+// memcpy reaches a fraction of host memory bandwidth, and the worker thread
+// must not spend launch time copying.
+class CopyPool {
+ public:
+  struct Copy {
+    void* dst;
+    const void* src;
+    size_t n;
+  };
+  explicit CopyPool(int nthreads) {
+    for (int i = 0; i < nthreads; ++i) th_.emplace_back([this] { loop(); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  // Runs every copy (split in pieces of at most kPiece bytes) and returns
+  // when all are done; the calling thread copies too.
+  void run(const std::vector<Copy>& copies) {
+    size_t total = 0;
+    for (const Copy& c : copies) total += c.n;
+    if (total < kParallelMin || th_.empty()) {
+      for (const Copy& c : copies) std::memcpy(c.dst, c.src, c.n);
+      return;
+    }
+    std::unique_lock<std::mutex> lk(mu_);
+    for (const Copy& c : copies)
+      for (size_t o = 0; o < c.n; o += kPiece)
+        work_.push_back(Copy{static_cast<uint8_t*>(c.dst) + o, static_cast<const uint8_t*>(c.src) + o,
+                             std::min(kPiece, c.n - o)});
+    pending_ += work_.size();
+    cv_.notify_all();
+    while (!work_.empty()) {
+      const Copy c = work_.front();
+      work_.pop_front();
+      lk.unlock();
+      std::memcpy(c.dst, c.src, c.n);
+      lk.lock();
+      --pending_;
+    }
+    done_cv_.wait(lk, [&] { return pending_ == 0; });
+  }
+
+ private:
+  static constexpr size_t kPiece = 1u << 20;
+  static constexpr size_t kParallelMin = 1u << 20;
+  void loop() {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return stop_ || !work_.empty(); });
+      if (stop_ && work_.empty()) return;
+      const Copy c = work_.front();
+      work_.pop_front();
+      lk.unlock();
+      std::memcpy(c.dst, c.src, c.n);
+      lk.lock();
+      if (--pending_ == 0) done_cv_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::deque<Copy> work_;
+  size_t pending_ = 0;
+  bool stop_ = false;
+};
+
 struct PlanEntry {
   fgfc_plan* plan = nullptr;
   int field = 0;
@@ -105,7 +177,7 @@ struct PlanEntry {
   std::vector<uint32_t> coeffs;
   uint64_t key = 0;
   int refs = 0;
-  uint64_t last = 0;
+  std::list<PlanEntry*>::iterator idle_pos;  // position in the idle list while refs == 0
 };
 
 uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
@@ -193,10 +265,13 @@ struct fgfc_server {
   bool stop = false;
   std::thread worker;
 
-  // plan cache (worker thread only)
+  // plan cache (worker thread only): unreferenced plans wait in `idle`,
+  // least recently used first, and are evicted from its front
   std::list<PlanEntry> plans;
+  std::list<PlanEntry*> idle;
   std::unordered_multimap<uint64_t, PlanEntry*> plan_index;
-  uint64_t use_clock = 0;
+  std::unique_ptr<CopyPool> copies;
+  std::unordered_map<uint64_t, std::vector<uint32_t>> decode_cache;  // rebuild requests (under mu)
 
   // statistics (under mu)
   std::vector<double> lat_us;
@@ -221,8 +296,7 @@ bool fgfc_server::acquire_plan(Req* r) {
   for (auto it = range.first; it != range.second; ++it) {
     PlanEntry* e = it->second;
     if (e->field == r->field && e->k == r->k && e->m == r->m && e->coeffs == r->coeffs) {
-      e->refs++;
-      e->last = ++use_clock;
+      if (e->refs++ == 0) idle.erase(e->idle_pos);
       r->plan = e;
       std::lock_guard<std::mutex> lk(mu);
       hits++;
@@ -230,19 +304,21 @@ bool fgfc_server::acquire_plan(Req* r) {
     }
   }
   // miss: evict least recently used unreferenced plans beyond the cache size
-  while (plans.size() >= cfg.plan_cache) {
-    auto victim = plans.end();
-    for (auto it = plans.begin(); it != plans.end(); ++it)
-      if (it->refs == 0 && (victim == plans.end() || it->last < victim->last)) victim = it;
-    if (victim == plans.end()) break;
+  while (plans.size() >= cfg.plan_cache && !idle.empty()) {
+    PlanEntry* victim = idle.front();
+    idle.pop_front();
     auto range2 = plan_index.equal_range(victim->key);
     for (auto it = range2.first; it != range2.second; ++it)
-      if (it->second == &*victim) {
+      if (it->second == victim) {
         plan_index.erase(it);
         break;
       }
     fgfc_plan_destroy(victim->plan);
-    plans.erase(victim);
+    for (auto it = plans.begin(); it != plans.end(); ++it)
+      if (&*it == victim) {
+        plans.erase(it);
+        break;
+      }
   }
   fgfc_plan* p = nullptr;
   if (fgfc_plan_create(static_cast<fgfc_field>(r->field), r->k, r->m, r->coeffs.data(), &p) != FGFC_OK) {
@@ -258,7 +334,6 @@ bool fgfc_server::acquire_plan(Req* r) {
   e.coeffs = r->coeffs;
   e.key = r->key;
   e.refs = 1;
-  e.last = ++use_clock;
   plan_index.emplace(e.key, &e);
   r->plan = &e;
   std::lock_guard<std::mutex> lk(mu);
@@ -267,7 +342,8 @@ bool fgfc_server::acquire_plan(Req* r) {
 }
 
 void fgfc_server::release_plan(Req* r) {
-  if (r->plan) r->plan->refs--;
+  PlanEntry* e = r->plan;
+  if (e && --e->refs == 0) e->idle_pos = idle.insert(idle.end(), e);
   r->plan = nullptr;
 }
 
@@ -333,12 +409,17 @@ void fgfc_server::issue(Launch* L) {
   uint8_t* sout = sbase + L->in_len;  // staged results: mirror of device [out0, out0 + out_len)
 
   cudaError_t e = cudaSuccess;
-  // stage inputs (CPU copies into page-locked memory), then one copy in
-  for (Req* r : L->reqs) {
-    if (!staged(r)) continue;
-    for (size_t t = 0; t < r->k; ++t) std::memcpy(sbase + r->d_src + t * r->Ls, r->src[t], r->L);
-    if (!r->ovr)
-      for (size_t j = 0; j < r->m; ++j) std::memcpy(sbase + r->d_rows + j * r->Ls, r->dst + r->starts[j], r->L);
+  // stage inputs (CPU copies into page-locked memory, split over the copy
+  // threads), then one copy in
+  {
+    std::vector<CopyPool::Copy> cp;
+    for (Req* r : L->reqs) {
+      if (!staged(r)) continue;
+      for (size_t t = 0; t < r->k; ++t) cp.push_back({sbase + r->d_src + t * r->Ls, r->src[t], r->L});
+      if (!r->ovr)
+        for (size_t j = 0; j < r->m; ++j) cp.push_back({sbase + r->d_rows + j * r->Ls, r->dst + r->starts[j], r->L});
+    }
+    copies->run(cp);
   }
   if (L->in_len) e = cudaMemcpyAsync(dbase, sbase, L->in_len, cudaMemcpyHostToDevice, s_in);
   for (Req* r : L->reqs) {
@@ -393,10 +474,12 @@ void fgfc_server::issue(Launch* L) {
 void fgfc_server::retire(Launch* L) {
   const uint8_t* sout = stg + L->stg_off + L->in_len;
   if (L->err == cudaSuccess) {
+    std::vector<CopyPool::Copy> cp;
     for (Req* r : L->reqs) {
       if (r->direct || r->on_device) continue;
-      for (size_t j = 0; j < r->m; ++j) std::memcpy(r->dst + r->starts[j], sout + (r->d_rows - L->out0) + j * r->Ls, r->L);
+      for (size_t j = 0; j < r->m; ++j) cp.push_back({r->dst + r->starts[j], sout + (r->d_rows - L->out0) + j * r->Ls, r->L});
     }
+    copies->run(cp);
   }
   for (Req* r : L->reqs) release_plan(r);
   std::lock_guard<std::mutex> lk(mu);
@@ -421,7 +504,10 @@ void fgfc_server::run_plain(Req* r) {
     // in place: exactly the call the request stands for
     std::vector<fgfc_slice> sl(r->k);
     for (size_t t = 0; t < r->k; ++t) sl[t] = fgfc_slice{r->src[t], r->L};
-    if (r->scattered)
+    if (r->scattered && r->ovr)
+      st = fgfc_dot_product_matrix_scattered_with(r->dst, r->dst_len, r->L, r->starts.data(), r->m, r->plan->plan,
+                                                  sl.data(), r->k, s_run);
+    else if (r->scattered)
       st = fgfc_mul_add_matrix_scattered_with(r->dst, r->dst_len, r->L, r->starts.data(), r->m, r->plan->plan,
                                               sl.data(), r->k, s_run);
     else if (r->ovr)
@@ -654,6 +740,7 @@ fgfc_status fgfc_server_create(const fgfc_server_config* cfg, fgfc_server** out)
   s->stg_arena.reset(s->cfg.staging_bytes);
   s->batch = batch_state_create();
   batch_state_graphs(s->batch, false);  // every launch has a new structure
+  s->copies = std::make_unique<CopyPool>(s->cfg.plain ? 0 : 7);
   s->worker = std::thread([p = s.get()] { p->run(); });
   *out = s.release();
   return clear_error();
@@ -692,22 +779,23 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
   r->dst_len = q->dst_len;
   const bool trivial = r->m == 0 || r->L == 0 || r->k == 0;
   if (!trivial) {
-    // all device memory of this server's device (used in place), or all host memory
+    // all device memory of this server's device (used in place), or all host
+    // memory; one attribute lookup per buffer (its first byte), plus the last
+    // byte of page-locked buffers long enough to be copied without staging
     int dev = -1, ndev = 0, nbuf = 0;
-    auto on_dev = [&](const void* p) {
+    bool locked = r->L >= kDirectMin;
+    auto look = [&](const void* p, size_t n) {
       ++nbuf;
-      if (where(p, &dev) == cudaMemoryTypeDevice && dev == s->device) ++ndev;
+      const cudaMemoryType t = where(p, &dev);
+      if (t == cudaMemoryTypeDevice && dev == s->device) ++ndev;
+      if (locked) locked = t == cudaMemoryTypeHost && host_locked(static_cast<const uint8_t*>(p) + n - 1);
     };
-    on_dev(r->dst);
-    for (size_t t = 0; t < r->k; ++t) on_dev(r->src[t]);
+    look(r->dst, q->dst_len);
+    for (size_t t = 0; t < r->k; ++t) look(r->src[t], r->L);
     if (ndev && ndev != nbuf)
       return set_error(FGFC_ERR_ARG, "server: a request's buffers must all be host memory or all device memory");
     r->on_device = ndev == nbuf;
-  }
-  if (!trivial && !r->on_device && r->L >= kDirectMin) {
-    bool locked = host_locked(r->dst) && host_locked(r->dst + q->dst_len - 1);
-    for (size_t t = 0; t < r->k && locked; ++t) locked = host_locked(r->src[t]) && host_locked(r->src[t] + r->L - 1);
-    r->direct = locked;
+    r->direct = !r->on_device && locked;
   }
   if (!trivial && (r->dev_bytes() > s->cfg.hbm_budget || r->stg_bytes() > s->cfg.staging_bytes))
     return set_error(FGFC_ERR_LIMIT, "server: request needs more device or staging memory than the server has");
@@ -739,6 +827,51 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
   s->pending.push_back(raw);
   s->cv.notify_all();
   return clear_error();
+}
+
+// A rebuild by erasure pattern: the decode rows of the pattern (host
+// Gauss-Jordan, decode.cpp; kept in a small cache keyed by a hash of the
+// code and the pattern) become the coefficients of an ordinary request that
+// overwrites the rebuilt shards.
+fgfc_status fgfc_server_submit_rebuild(fgfc_server* s, const fgfc_rebuild_request* q, uint64_t* ticket) {
+  if (!s || !q || !ticket) return set_error(FGFC_ERR_ARG, "server: null argument");
+  if (field_bytes(q->field) == 0) return set_error(FGFC_ERR_ARG, "server: unknown field");
+  if (!q->k || !q->survivors || !q->parity || (q->nerased && !q->erased))
+    return set_error(FGFC_ERR_ARG, "server: rebuild request without code or pattern");
+  uint64_t h = 0xcbf29ce484222325ull;
+  h = fnv1a(h, &q->field, sizeof q->field);
+  h = fnv1a(h, &q->k, sizeof q->k);
+  h = fnv1a(h, &q->m, sizeof q->m);
+  h = fnv1a(h, q->parity, q->m * q->k * sizeof(uint32_t));
+  h = fnv1a(h, q->survivors, q->k * sizeof(size_t));
+  h = fnv1a(h, q->erased, q->nerased * sizeof(size_t));
+  std::vector<uint32_t> d;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->decode_cache.find(h);
+    if (it != s->decode_cache.end()) d = it->second;
+  }
+  if (d.empty()) {
+    d.resize(q->k * q->nerased + 1);
+    const fgfc_status st =
+        decode_matrix(q->field, q->parity, q->k, q->m, q->survivors, q->erased, q->nerased, d.data());
+    if (st != FGFC_OK) return st;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->decode_cache.size() >= 4096) s->decode_cache.clear();
+    s->decode_cache.emplace(h, d);
+  }
+  fgfc_request r;
+  r.field = q->field;
+  r.coeffs = d.data();
+  r.srcs = q->srcs;
+  r.nsrcs = q->k;
+  r.dst = q->dst;
+  r.dst_len = q->dst_len;
+  r.row_starts = q->row_starts;
+  r.nrows = q->nerased;
+  r.row_len = q->row_len;
+  r.overwrite = 1;
+  return fgfc_server_submit(s, &r, ticket);
 }
 
 fgfc_status fgfc_server_poll(fgfc_server* s, uint64_t ticket, int* done) {

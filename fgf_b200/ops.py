@@ -111,6 +111,18 @@ class Plan:
         return cls(field, coeffs)
 
     @classmethod
+    def _adopt(cls, field, handle: C.c_void_p, rows: int, cols: int) -> "Plan":
+        """Wrap a plan the library created (e.g. fgfc_decode_plan_create)."""
+        self = cls.__new__(cls)
+        self.field = FIELDS[_fid(field)]
+        self._h = handle
+        vals = (C.c_uint32 * max(1, rows * cols))()
+        check(lib().fgfc_plan_values(handle, vals))
+        self._values = list(vals[:rows * cols])
+        self._rows, self._cols = rows, cols
+        return self
+
+    @classmethod
     def matrix(cls, field, rows: int, cols: int, coeffs: Sequence[int]) -> "Plan":
         if rows * cols != len(coeffs):
             # ops.rs:199-207 (the C ABI reports the same condition; checked

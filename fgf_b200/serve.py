@@ -14,7 +14,7 @@ from __future__ import annotations
 import ctypes as C
 from typing import Sequence
 
-from ._lib import Request, ServerConfig, ServerStats, Slice, check, lib
+from ._lib import RebuildRequest, Request, ServerConfig, ServerStats, Slice, check, lib
 from .ops import _fid
 
 
@@ -79,6 +79,31 @@ class Server:
         """Enqueue one call; its buffers must stay untouched until it completes."""
         return self.submit_prepared(PreparedRequest(field, coeffs, srcs, dst, row_len, nrows, overwrite,
                                                     row_starts))
+
+    def submit_rebuild(self, field, parity: Sequence[Sequence[int]], survivors: Sequence[int], srcs: Sequence,
+                       erased: Sequence[int], dst, row_len: int, row_starts: Sequence[int] | None = None) -> int:
+        """Rebuild shards `erased` of the code [I_k ; parity] from the survivor
+        shards `srcs` (indices `survivors`), written over dst; the server
+        derives and caches the decode rows."""
+        m, k = len(parity), len(survivors)
+        flat = (C.c_uint32 * max(1, m * k))(*[int(v) for row in parity for v in row])
+        sv = (C.c_size_t * max(1, k))(*[int(x) for x in survivors])
+        er = (C.c_size_t * max(1, len(erased)))(*[int(x) for x in erased])
+        bufs = [_host(x) for x in srcs]
+        sl = (Slice * max(1, len(bufs)))(*[Slice(p, n) for p, n, _ in bufs])
+        d, dn, downer = _host(dst)
+        rs = None
+        if row_starts is not None:
+            rs = (C.c_size_t * max(1, len(row_starts)))(*[int(v) for v in row_starts])
+        q = RebuildRequest(_fid(field), C.cast(flat, C.POINTER(C.c_uint32)), k, m, C.cast(sv, C.POINTER(C.c_size_t)),
+                           C.cast(sl, C.POINTER(Slice)), C.cast(er, C.POINTER(C.c_size_t)), len(erased), d, dn,
+                           C.cast(rs, C.POINTER(C.c_size_t)) if rs is not None else None, int(row_len))
+        t = C.c_uint64()
+        check(lib().fgfc_server_submit_rebuild(self._h, C.byref(q), C.byref(t)))
+        keep = PreparedRequest.__new__(PreparedRequest)
+        keep.keep = [flat, sv, er, sl, rs, downer] + [o for _, _, o in bufs]
+        self._live[t.value] = keep
+        return t.value
 
     def submit_prepared(self, req: PreparedRequest) -> int:
         t = C.c_uint64()

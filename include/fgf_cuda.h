@@ -205,6 +205,34 @@ fgfc_status fgfc_dot_product_matrix_scattered_with(uint8_t *dst, size_t dst_len,
                                                    const fgfc_plan *plan, const fgfc_slice *srcs,
                                                    size_t nsrcs, fgfc_stream stream);
 
+/* ---------------------------------------------------------------- coding and decode matrices */
+
+/* No counterpart in the crate, which leaves coding-matrix construction to its
+ * callers (src/lib.rs:115-116); the recipes of its round-trip test
+ * (tests/ops.rs:897-950) with its inv(0) = 0 convention (src/field/mod.rs:38-41).
+ * Host computation; no device work. */
+
+/* Cauchy parity matrix, row-major m x k: out[i * k + j] = inv(x_i + y_j),
+ * x_i = x0 + i, y_j = j. FGFC_ERR_ARG if some x_i + y_j is zero or a value
+ * does not fit the field. */
+fgfc_status fgfc_cauchy_matrix(fgfc_field field, size_t m, size_t k, uint32_t x0, uint32_t *out);
+/* Decode rows of the systematic code [I_k ; C] (`parity` = C, row-major
+ * m x k): with k distinct surviving shard indices (0..k-1 data, k..k+m-1
+ * parity) and `nerased` shard indices to rebuild, out (k x nerased,
+ * term-major: out[t * nerased + e]) satisfies
+ * shard[erased[e]] = sum_t out[t * nerased + e] * shard[survivors[t]], the
+ * layout Plan::matrix(k, nerased) takes. The survivor submatrix is inverted
+ * by Gauss-Jordan elimination over the field; FGFC_ERR_ARG if it is
+ * singular or an index is out of range or repeated. */
+fgfc_status fgfc_decode_matrix(fgfc_field field, const uint32_t *parity, size_t k, size_t m,
+                               const size_t *survivors, const size_t *erased, size_t nerased,
+                               uint32_t *out);
+/* The same decode rows as a prepared plan of dimensions (k, nerased), ready
+ * for mul_add_matrix_scattered_with / dot_product_matrix_scattered_with. */
+fgfc_status fgfc_decode_plan_create(fgfc_field field, const uint32_t *parity, size_t k, size_t m,
+                                    const size_t *survivors, const size_t *erased, size_t nerased,
+                                    fgfc_plan **out);
+
 /* ---------------------------------------------------------------- batches */
 
 /* One stripe of a batched submission: the arguments of one
@@ -332,6 +360,10 @@ int fgfc_tune_usable(fgfc_kernel kernel, fgfc_field field, size_t nsrcs, size_t 
  * on the current device (allocates and frees its own buffers) and records the
  * fastest for the shape's row-length bucket; the winner goes to *out. */
 fgfc_status fgfc_tune_shape(fgfc_field field, size_t nsrcs, size_t nrows, size_t row_len, fgfc_kernel *out);
+/* Error word of the current device's tensor-core kernels, whose waits are
+ * bounded: FGFC_ERR_CUDA if one gave up (its call's results are then not
+ * valid), else FGFC_OK. Synchronises with the device; `clear` resets it. */
+fgfc_status fgfc_device_check(int clear);
 fgfc_status fgfc_tune_save(const char *path);
 fgfc_status fgfc_tune_load(const char *path);
 void fgfc_tune_clear(void);
@@ -353,7 +385,8 @@ void fgfc_tune_clear(void);
  * device plans once and cached, keyed by a hash of (field, dimensions,
  * coefficients). Request buffers in page-locked host memory with rows of at
  * least 256 KiB are copied directly; other host buffers go through the
- * server's page-locked staging buffers. A request whose buffers are all
+ * server's page-locked staging buffers, filled and emptied by a small pool of
+ * host copy threads. A request whose buffers are all
  * device memory of the server's device runs in place, without copies (a
  * request mixing host and device buffers is rejected with FGFC_ERR_ARG). */
 typedef struct fgfc_server fgfc_server;
@@ -403,6 +436,28 @@ fgfc_status fgfc_server_create(const fgfc_server_config *cfg, fgfc_server **out)
  * copied, the host shards and dst must stay valid and untouched until the
  * request completes. FGFC_ERR_LIMIT if it can never fit the budgets. */
 fgfc_status fgfc_server_submit(fgfc_server *server, const fgfc_request *req, uint64_t *ticket);
+/* A rebuild by erasure pattern: `srcs` hold the k survivor shards
+ * `survivors` (indices into the code [I_k ; parity], parity row-major m x k)
+ * and shard erased[e] is written over dst + row_starts[e] (row_starts NULL:
+ * e * row_len). The server computes the decode rows itself
+ * (fgfc_decode_matrix), caches them by pattern, and runs the request as the
+ * overwrite form of mul_add_matrix_scattered. Same buffer rules as
+ * fgfc_server_submit. */
+typedef struct fgfc_rebuild_request {
+  fgfc_field field;
+  const uint32_t *parity;   /* m x k, row-major */
+  size_t k, m;
+  const size_t *survivors;  /* k shard indices, in the order of srcs */
+  const fgfc_slice *srcs;   /* k survivor shards, row_len bytes each */
+  const size_t *erased;     /* nerased shard indices to rebuild */
+  size_t nerased;
+  uint8_t *dst;
+  size_t dst_len;
+  const size_t *row_starts; /* nerased offsets into dst, or NULL */
+  size_t row_len;
+} fgfc_rebuild_request;
+fgfc_status fgfc_server_submit_rebuild(fgfc_server *server, const fgfc_rebuild_request *req,
+                                       uint64_t *ticket);
 /* Blocks until the request is done and returns its status (its message via
  * fgfc_last_error); a ticket can be waited for once. */
 fgfc_status fgfc_server_wait(fgfc_server *server, uint64_t ticket);

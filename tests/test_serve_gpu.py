@@ -192,3 +192,73 @@ def test_device_resident_requests_run_in_place(cuda):
         with pytest.raises(FgfError) as e:
             srv.submit(Gf8D, [1], [torch.zeros(64, dtype=torch.uint8, device="cuda")], np.zeros(64, np.uint8), 64, 1)
         assert e.value.status == 11
+
+
+def test_rebuild_requests_by_erasure_pattern(cuda):
+    """fgfc_server_submit_rebuild: the server derives the decode rows of each
+    pattern; rebuilt shards (written over garbage) equal the originals, for
+    host and device buffers, alone and batched together."""
+    from fgf_b200 import codes
+
+    k, m, L = 10, 4, 65536 + 32
+    parity = codes.cauchy_matrix(Gf8D, m, k)
+    vals = [parity[i][t] for t in range(k) for i in range(m)]
+    data = [orc.noise(L, 0xBE + t) for t in range(k)]
+    shards = data + [np.zeros(L, np.uint8) for _ in range(m)]
+    want = np.zeros(m * L, np.uint8)
+    orc.dot_product_matrix(Gf8D.ID, want, L, m, vals, data)
+    for j in range(m):
+        shards[k + j] = want[j * L:(j + 1) * L].copy()
+    rng = np.random.default_rng(77)
+    patterns = [sorted(int(x) for x in rng.choice(k + m, size=m, replace=False)) for _ in range(12)]
+    for where in ("host", "device"):
+        srv = serve.Server(hbm_budget=1 << 30, staging_bytes=256 << 20)
+        try:
+            jobs = []
+            for er in patterns:
+                sv = [i for i in range(k + m) if i not in er][:k]
+                if where == "host":
+                    srcs = [shards[i] for i in sv]
+                    out = np.full(m * L, 0xEE, np.uint8)
+                else:
+                    srcs = [torch.from_numpy(shards[i]).cuda() for i in sv]
+                    out = torch.full((m * L,), 0xEE, dtype=torch.uint8, device="cuda")
+                t = srv.submit_rebuild(Gf8D, parity, sv, srcs, er, out, L)
+                jobs.append((t, er, out, srcs))
+            for t, er, out, _ in jobs:
+                srv.wait(t)
+                got = out if where == "host" else out.cpu().numpy()
+                for j, e in enumerate(er):
+                    assert np.array_equal(got[j * L:(j + 1) * L], shards[e]), f"{where}: pattern {er} shard {e}"
+            st = srv.stats()
+            assert st["completed"] == len(patterns)
+        finally:
+            srv.close()
+
+
+def test_overwrite_scattered_through_batch_and_single_call(cuda):
+    """dot_product_matrix_scattered_with (batch job with row_starts and
+    overwrite): equals zeroing the rows, then mul_add_matrix_scattered."""
+    from fgf_b200 import batch as fb
+    from fgf_b200 import ops
+
+    rng = np.random.default_rng(78)
+    for field, k, m, L in ((Gf8D, 10, 4, 65536 + 5), (Gf16, 6, 3, 2 * 5001), (Gf32, 4, 2, 4 * 1003)):
+        coeffs = [int(x) for x in rng.integers(0, 1 << (8 * field.BYTES), size=k * m, dtype=np.uint64)]
+        srcs_h = [rng.integers(0, 256, size=L, dtype=np.uint8) for _ in range(k)]
+        gap = L + 3 * field.BYTES
+        starts = [j * gap for j in range(m)][::-1]
+        init = rng.integers(0, 256, size=gap * m + 8, dtype=np.uint8)
+        want = init.copy()
+        for st in starts:
+            want[st:st + L] = 0
+        orc.mul_add_matrix_scattered(field.ID, want, L, starts, coeffs, srcs_h)
+        plan = ops.Plan.matrix(field, k, m, coeffs)
+        srcs = [torch.from_numpy(s).cuda() for s in srcs_h]
+        d1 = torch.from_numpy(init.copy()).cuda()
+        ops.dot_product_matrix_scattered_with(d1, L, starts, plan, srcs)
+        d2 = torch.from_numpy(init.copy()).cuda()
+        fb.Batch().run([fb.Job(plan, srcs, d2, L, m, True, starts)])
+        torch.cuda.synchronize()
+        assert np.array_equal(d1.cpu().numpy(), want), field.__name__
+        assert np.array_equal(d2.cpu().numpy(), want), field.__name__
