@@ -56,7 +56,8 @@ constexpr uint32_t kCols = 512;        // element columns per block (4 tiles of 
 constexpr uint32_t kMaxInBits = 512;   // K
 constexpr uint32_t kMaxOutBits = 128;  // N
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s: a wait this long means the pipeline is stuck
+constexpr uint64_t kDrainNs = 1000000000ull;  // 1 s per drain wait before the CTA exits
 
 struct Gf2Launch {
   const uint8_t* src[kMaxSrc];  // kMaxSrc >= 64 sources
@@ -100,14 +101,26 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; false when it ran out. With `honor_abort` it also gives up
-// once another role has aborted (the drain waits before exit do not).
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait bounded in time (every wait of a correct run lasts microseconds);
+// false when it ran out. With `honor_abort` it also gives up once another
+// role has aborted (the drain waits before exit do not).
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, bool honor_abort = true) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+  if (mbar_try(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  const uint64_t limit = honor_abort ? kWaitNs : kDrainNs;
+  for (uint32_t i = 1;; ++i) {
     if (mbar_try(b, parity)) return true;
-    if (honor_abort && (i & 1023u) == 1023u && *abort) return false;
+    if ((i & 255u) == 0) {
+      if (honor_abort && *abort) return false;
+      if (global_ns() - t0 > limit) return false;
+    }
   }
-  return false;
 }
 
 // The same wait by every lane of a warp, with a warp-uniform result (the

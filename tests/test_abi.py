@@ -32,3 +32,21 @@ def test_library_exports_every_declared_symbol():
 
 def test_binding_covers_the_header():
     assert declared("fgf_cuda.h") <= set(_lib.declared_symbols())
+
+
+def test_rust_crate_binds_every_entry_point():
+    """The fgf-cuda crate (source only here: no cargo in this image) declares
+    every C-ABI entry point in sys.rs and mirrors every public fgf::ops
+    function (src/ops.rs:323-1017) in ops.rs."""
+    crate = ROOT / "fgf_b200" / "rust" / "fgf-cuda" / "src"
+    sys_rs = (crate / "sys.rs").read_text()
+    bound = set(re.findall(r"pub fn (fgfc_[a-z0-9_]+)\s*\(", sys_rs))
+    missing = declared("fgf_cuda.h") - bound
+    assert not missing, f"sys.rs lacks {sorted(missing)}"
+    ops_rs = (crate / "ops.rs").read_text()
+    wrapped = set(re.findall(r"pub fn ([a-z_]+)<F: CudaField>", ops_rs))
+    for op in ("add_assign", "sub_assign", "mul_add", "mul_add_with", "mul_into", "mul_into_with", "mul_assign",
+               "mul_assign_with", "mul_elementwise", "mul_add_scatter", "mul_add_scatter_with", "mul_add_gather",
+               "mul_add_gather_with", "dot_product", "dot_product_with", "mul_add_matrix", "mul_add_matrix_with",
+               "dot_product_matrix", "dot_product_matrix_with", "mul_add_matrix_scattered"):
+        assert op in wrapped, f"ops.rs lacks {op}"
