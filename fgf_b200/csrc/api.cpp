@@ -84,6 +84,7 @@ struct fgfc_plan {
   // rows x cols; scatter: 1 x len; gather: len x 1), empty where the shape
   // is outside that kernel's range
   std::vector<uint32_t> bits_mat, bits_scat, bits_gath;
+  uint64_t bits_key = 0;  // hash of bits_mat
   int device;
   uint32_t* dev;        // device tables, three orientations back to back
   size_t mat_groups;    // groups per source in the matrix orientation
@@ -267,6 +268,9 @@ fgfc_status upload_plan_tables(fgfc_plan* p) {
   if (n_mat && gf2mma_shape_ok(p->field, p->rows, p->cols)) {
     p->bits_mat.resize(kGf2BitWords);
     gf2mma_bits(p->field, p->values.data(), p->rows, p->cols, p->bits_mat.data());
+    uint64_t h = 1469598103934665603ull ^ (static_cast<uint64_t>(p->field) << 56);
+    for (uint32_t w : p->bits_mat) h = (h ^ w) * 1099511628211ull;
+    p->bits_key = h;
   }
   if (len && gf2mma_shape_ok(p->field, 1, len)) {
     p->bits_scat.resize(kGf2BitWords);
@@ -906,13 +910,15 @@ struct fgfc_batch {
 
 namespace fgfc {
 
+namespace {
+
 // One stripe (all sources of a plan, rows at the given device addresses) as
-// sub-jobs of at most 4 table groups. The vector body is used when every
+// table sub-jobs of at most 4 groups. The vector body is used when every
 // source has the same offset within 16 bytes (a multiple of the element
 // size), whatever the rows' offsets; otherwise the whole stripe takes the
 // 4-byte-group path.
-void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
-                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out) {
+void lower_tables(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
+                  size_t row_len, bool overwrite, std::vector<LoweredJob>& out) {
   const int field = plan->field;
   const int E = field_bytes(field);
   const int R = 4 / E;
@@ -946,6 +952,49 @@ void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, 
       for (uint64_t d : L.dsts) L.shift = L.shift || (d & 15) != al;
     out.push_back(std::move(L));
   }
+}
+
+std::vector<uint64_t> offset_by(const std::vector<uint64_t>& p, uint64_t off) {
+  std::vector<uint64_t> out(p);
+  for (auto& x : out) x += off;
+  return out;
+}
+
+}  // namespace
+
+void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
+                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out, std::vector<Gf2Job>& tc) {
+  const int field = plan->field;
+  const int E = field_bytes(field);
+  const size_t k = srcs.size(), m = dsts.size();
+  const size_t blk_bytes = 512 * static_cast<size_t>(E);
+  if (k && m && !plan->bits_mat.empty() && choose_kernel(field, k, m, row_len) == FGFC_KERNEL_GF2MMA) {
+    const uint64_t al = srcs[0] & 15;
+    bool same = al % E == 0;
+    for (uint64_t p : srcs) same = same && (p & 15) == al;
+    for (uint64_t p : dsts) same = same && (p & 15) == al;
+    const uint64_t head = std::min<uint64_t>((16 - al) & 15, row_len);
+    const uint64_t nblk = same ? (row_len - head) / blk_bytes : 0;
+    if (nblk) {
+      Gf2Job J;
+      J.field = field;
+      J.bits = plan->bits_mat.data();
+      J.bits_key = plan->bits_key;
+      J.k = k;
+      J.m = m;
+      J.ovr = overwrite;
+      J.nblk = nblk;
+      J.ptrs = offset_by(srcs, head);
+      const std::vector<uint64_t> d = offset_by(dsts, head);
+      J.ptrs.insert(J.ptrs.end(), d.begin(), d.end());
+      tc.push_back(std::move(J));
+      if (head) lower_tables(plan, srcs, dsts, head, overwrite, out);
+      const uint64_t end = head + nblk * blk_bytes;
+      if (end < row_len) lower_tables(plan, offset_by(srcs, end), offset_by(dsts, end), row_len - end, overwrite, out);
+      return;
+    }
+  }
+  lower_tables(plan, srcs, dsts, row_len, overwrite, out);
 }
 
 }  // namespace fgfc
@@ -984,6 +1033,7 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
                            fgfc_stream stream) {
   if (!batch || (njobs && !jobs)) return fail(FGFC_ERR_ARG, "batch: null argument");
   std::vector<LoweredJob> low;
+  std::vector<Gf2Job> tc;
   low.reserve(njobs);
   for (size_t i = 0; i < njobs; ++i) {
     const fgfc_matrix_job& J = jobs[i];
@@ -1035,9 +1085,9 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
       dsts[j] = reinterpret_cast<uint64_t>(J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len));
     std::vector<uint64_t> srcs(J.nsrcs);
     for (size_t t = 0; t < J.nsrcs; ++t) srcs[t] = reinterpret_cast<uint64_t>(J.srcs[t].ptr);
-    lower_matrix_job(plan, srcs, dsts, J.row_len, J.overwrite != 0, low);
+    lower_matrix_job(plan, srcs, dsts, J.row_len, J.overwrite != 0, low, tc);
   }
-  cudaError_t e = batch_run(batch->state, low, stream);
+  cudaError_t e = batch_run(batch->state, low, tc, stream);
   return e == cudaSuccess ? ok() : cuda_fail(e, "batch");
 }
 

@@ -29,6 +29,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/fgf_cuda.h"
@@ -636,12 +637,13 @@ void batch_state_stats(const void* p, size_t* launches, size_t* items, int* repl
 
 static size_t align16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
 
-cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream) {
+cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const std::vector<Gf2Job>& tc,
+                      cudaStream_t stream) {
   BatchState* b = static_cast<BatchState*>(state);
   std::lock_guard<std::mutex> lk(b->mu);
   b->last_launches = b->last_items = 0;
   b->last_replayed = 0;
-  if (jobs.empty()) return cudaSuccess;
+  if (jobs.empty() && tc.empty()) return cudaSuccess;
 
   // ---- device descriptors, pointer array, classes (sub-jobs in plan order)
   std::vector<BatchJob> dj(jobs.size());
@@ -726,6 +728,36 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     }
     cb.push_back(x);
   }
+  // tensor-core bodies: one launch per plan (bit matrix), its stripes'
+  // pointers and first blocks in the blob
+  struct TcGroup {
+    std::vector<size_t> idx;
+    size_t off_ptrs = 0, off_prefix = 0;
+    uint64_t nblk = 0;
+  };
+  std::vector<TcGroup> tcg;
+  {
+    std::map<std::tuple<uint64_t, int, size_t, size_t, bool>, size_t> gi;
+    for (size_t i = 0; i < tc.size(); ++i) {
+      const Gf2Job& J = tc[i];
+      const auto key = std::make_tuple(J.bits_key, J.field, J.k, J.m, J.ovr);
+      auto it = gi.find(key);
+      if (it == gi.end()) {
+        it = gi.emplace(key, tcg.size()).first;
+        tcg.emplace_back();
+      }
+      TcGroup& G = tcg[it->second];
+      G.idx.push_back(i);
+      G.nblk += J.nblk;
+    }
+    for (TcGroup& G : tcg) {
+      const Gf2Job& J0 = tc[G.idx[0]];
+      G.off_ptrs = off;
+      off = align16(off + G.idx.size() * (J0.k + J0.m) * sizeof(uint64_t));
+      G.off_prefix = off;
+      off = align16(off + (G.idx.size() + 1) * sizeof(uint64_t));
+    }
+  }
   const size_t bytes = off;
 
   BatchSlot& s = b->slot[b->next];
@@ -747,6 +779,20 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
       std::memcpy(s.host + x.first, kv.second.items.data(), kv.second.items.size() * sizeof(uint2));
       std::memset(s.host + x.second, 0, 64);
     }
+    for (const TcGroup& G : tcg) {
+      uint64_t* hp = reinterpret_cast<uint64_t*>(s.host + G.off_ptrs);
+      uint64_t* pre = reinterpret_cast<uint64_t*>(s.host + G.off_prefix);
+      uint64_t acc = 0;
+      size_t n = 0;
+      for (size_t i : G.idx) {
+        const Gf2Job& J = tc[i];
+        std::memcpy(hp, J.ptrs.data(), J.ptrs.size() * sizeof(uint64_t));
+        hp += J.ptrs.size();
+        pre[n++] = acc;
+        acc += J.nblk;
+      }
+      pre[n] = acc;
+    }
   }
 
   // ---- launches (their structure is the graph key)
@@ -759,6 +805,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     uint32_t n = 0;
     uint32_t* counter = nullptr;
     size_t uparam = 0;
+    int tc_group = -1;  // >= 0: a tensor-core launch over that group's stripes
   };
   std::vector<Launch> launches;
   std::vector<UniformParams>& uparams = b->uparams;
@@ -831,6 +878,18 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
       launches.push_back(L);
     }
   }
+  for (size_t g = 0; g < tcg.size(); ++g) {
+    const Gf2Job& J0 = tc[tcg[g].idx[0]];
+    e = gf2mma_prepare(field_bytes(J0.field));  // before any capture records the launch
+    if (e != cudaSuccess) return e;
+    Launch L;
+    L.tc_group = static_cast<int>(g);
+    b->last_items += tcg[g].idx.size();
+    key += "|g" + std::to_string(J0.bits_key) + "," + std::to_string(J0.field) + "," + std::to_string(J0.k) + "," +
+           std::to_string(J0.m) + "," + std::to_string(J0.ovr) + "," + std::to_string(tcg[g].idx.size()) + "," +
+           std::to_string(tcg[g].nblk);
+    launches.push_back(L);
+  }
   const BatchJob* djobs = reinterpret_cast<const BatchJob*>(s.dev + off_jobs);
   const uint64_t* dptrs = reinterpret_cast<const uint64_t*>(s.dev + off_ptrs);
 
@@ -859,11 +918,19 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStre
     for (size_t li = 0; li < launches.size(); ++li) {
       const Launch& L = launches[li];
       cudaStream_t ls = nside ? b->side[li % nside] : st;
-      if (L.ufn)
+      if (L.tc_group >= 0) {
+        const TcGroup& G = tcg[L.tc_group];
+        const Gf2Job& J0 = tc[G.idx[0]];
+        err = gf2mma_launch_multi(J0.field, J0.k, J0.m, J0.bits, reinterpret_cast<const uint64_t*>(s.dev + G.off_ptrs),
+                                  reinterpret_cast<const uint64_t*>(s.dev + G.off_prefix),
+                                  static_cast<uint32_t>(G.idx.size()), G.nblk, J0.ovr, ls);
+      } else if (L.ufn) {
         L.ufn<<<L.grid, L.threads, L.smem, ls>>>(uparams[L.uparam]);
-      else
+        err = cudaGetLastError();
+      } else {
         L.fn<<<L.grid, L.threads, L.smem, ls>>>(djobs, dptrs, L.items, L.n, L.counter);
-      err = cudaGetLastError();
+        err = cudaGetLastError();
+      }
       if (err != cudaSuccess) return err;
     }
     for (int i = 0; i < nside && err == cudaSuccess; ++i) {

@@ -56,8 +56,13 @@ constexpr uint32_t kCols = 512;        // element columns per block (4 tiles of 
 constexpr uint32_t kMaxInBits = 512;   // K
 constexpr uint32_t kMaxOutBits = 128;  // N
 constexpr uint32_t kTmemCols = 512;
+constexpr int kMaxLaunchSmem = 227 * 1024;  // the opt-in every launch fits under
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s: a wait this long means the pipeline is stuck
 constexpr uint64_t kDrainNs = 1000000000ull;  // 1 s per drain wait before the CTA exits
+
+// Error word of this device's launches (0 = fine): a bounded wait that ran
+// out records where. Read and cleared by gf2mma_error.
+__device__ int g_gf2_err;
 
 struct Gf2Launch {
   const uint8_t* src[kMaxSrc];  // kMaxSrc >= 64 sources
@@ -67,7 +72,12 @@ struct Gf2Launch {
   uint32_t ngroups;             // K / 32: groups of 4 input bytes
   uint32_t npad;                // N: output bits padded to a multiple of 16
   uint32_t overwrite;
-  int* err;                     // device error word (0 = fine)
+  // Several stripes sharing this plan (nstripes > 0): stripe s owns blocks
+  // [prefix[s], prefix[s + 1]) and its k source and m row pointers are
+  // ptrs[s * (k + m) ..]; with nstripes == 0 the single stripe is src / dst.
+  const uint64_t* ptrs;
+  const uint64_t* prefix;
+  uint32_t nstripes;
   // bits[n][g]: bit (8r + b) set iff output bit n takes input byte 4g + r, bit b
   uint32_t bits[kMaxOutBits][kMaxInBits / 32];
 };
@@ -204,6 +214,20 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
+// The stripe of a block. A CTA meets its blocks in increasing order, so the
+// cursor only walks forward.
+struct StripeCursor {
+  uint32_t s = 0;
+  // Address of column block `blk` of source t (t < k) or row t - k.
+  template <int E>
+  __device__ __forceinline__ uint8_t* at(const Gf2Launch& a, uint64_t blk, uint32_t t) {
+    if (!a.nstripes) return (t < a.k ? const_cast<uint8_t*>(a.src[t]) : a.dst[t - a.k]) + blk * kCols * E;
+    while (s + 1 < a.nstripes && a.prefix[s + 1] <= blk) ++s;
+    return reinterpret_cast<uint8_t*>(a.ptrs[static_cast<uint64_t>(s) * (a.k + a.m) + t]) +
+           (blk - a.prefix[s]) * kCols * E;
+  }
+};
+
 // Output byte from 8 accumulators (bit o of the byte = bit 7 of r[o]).
 __device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
   const uint32_t p03 = prmt(prmt(r[0], r[1], 0x0040u), prmt(r[2], r[3], 0x0040u), 0x5410u);
@@ -224,7 +248,7 @@ struct Smem {
 // column q (byte q of out[v]); after the 4th tile store 4 columns of every row.
 template <int E, int Q>
 __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
-                                         uint32_t (&out)[16], volatile int* abort) {
+                                         uint32_t (&out)[16], volatile int* abort, StripeCursor& cur) {
   constexpr uint32_t b = Q & 1;
   constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
   const uint32_t warp = threadIdx.x >> 5, i = threadIdx.x;
@@ -251,11 +275,11 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
   }
   if (Q == 3) {
     const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
-    const uint64_t off = blk * kCols * E + static_cast<uint64_t>(i) * 4u * E;
+    const uint64_t off = static_cast<uint64_t>(i) * 4u * E;
 #pragma unroll
     for (uint32_t j = 0; j < 16 / E; ++j) {
       if (j >= a.m) break;
-      uint8_t* p = a.dst[j] + off;
+      uint8_t* p = cur.at<E>(a, blk, a.k + j) + off;
       if (E == 1) {
         uint32_t v = out[j];
         if (!a.overwrite) v ^= *reinterpret_cast<const uint32_t*>(p);
@@ -341,6 +365,7 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
   for (int x = 0; x < 16; ++x) out[x] = 0;
   const uint32_t nwords = a.k * E;
   bool ok = true;
+  StripeCursor cur;
   uint64_t t = 0;  // tiles expanded so far
   for (uint64_t it = 0; it < nmine && ok; ++it) {
     const uint32_t s = static_cast<uint32_t>(it % kStages);
@@ -372,7 +397,7 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     // tile Q of this block is tile t + Q; before it reuses buffer Q % 2, the
     // tile two before it (t + Q - 2) is read back
 #define FGFC_TILE(Q, PQ)                                                      \
-    if (ok && t + Q >= 2) ok = epilogue<E, PQ>(a, S, d_col, t + Q - 2, out, abort); \
+    if (ok && t + Q >= 2) ok = epilogue<E, PQ>(a, S, d_col, t + Q - 2, out, abort, cur); \
     if (ok) {                                                                 \
       expand<E, Q>(a, sw, a_col[Q & 1]);                                      \
       tc_fence_before();                                                      \
@@ -387,10 +412,10 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     t += 4;
   }
   // the last two tiles (columns 2 and 3 of the last block)
-  if (ok && t >= 2) ok = epilogue<E, 2>(a, S, d_col, t - 2, out, abort);
-  if (ok && t >= 2) ok = epilogue<E, 3>(a, S, d_col, t - 1, out, abort);
+  if (ok && t >= 2) ok = epilogue<E, 2>(a, S, d_col, t - 2, out, abort, cur);
+  if (ok && t >= 2) ok = epilogue<E, 3>(a, S, d_col, t - 1, out, abort, cur);
   if (!ok) {
-    atomicExch(a.err, 3);
+    atomicExch(&g_gf2_err, 3);
     *abort = 1;
   }
   (void)nwords;
@@ -465,17 +490,18 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
     uint64_t issued = 0;
     if (lane == 0) {
       const uint32_t row_bytes = kCols * E;
+      StripeCursor cur;
       for (uint64_t i = 0; i < nmine && !*abort; ++i) {
         const uint32_t s = static_cast<uint32_t>(i % kStages);
         if (i >= kStages && !mbar_wait(&S.empty[s], static_cast<uint32_t>((i / kStages - 1) & 1u), abort)) {
-          atomicExch(a.err, 1);
+          atomicExch(&g_gf2_err, 1);
           *abort = 1;
           break;
         }
         const uint64_t blk = blockIdx.x + i * gridDim.x;
         mbar_expect_tx(&S.full[s], a.k * row_bytes);
         for (uint32_t t = 0; t < a.k; ++t)
-          bulk_g2s(stages + s * stage_bytes + t * row_bytes, a.src[t] + blk * row_bytes, row_bytes, &S.full[s]);
+          bulk_g2s(stages + s * stage_bytes + t * row_bytes, cur.at<E>(a, blk, t), row_bytes, &S.full[s]);
         ++issued;
       }
       // copies still in flight must land before the CTA exits
@@ -492,7 +518,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       for (; t < ntiles && !*abort; ++t) {
         const uint32_t b = static_cast<uint32_t>(t & 1u);
         if (!mbar_wait(&S.afull[b], static_cast<uint32_t>((t >> 1) & 1u), abort)) {
-          atomicExch(a.err, 2);
+          atomicExch(&g_gf2_err, 2);
           *abort = 1;
           break;
         }
@@ -514,22 +540,6 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   tc_fence_after();
   if (warp == 5)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
-}
-
-// Per-device error word for the kernel's bounded waits.
-int* error_word() {
-  static std::mutex mu;
-  static int* words[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> lk(mu);
-  if (!words[dev]) {
-    int* p = nullptr;
-    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
-    cudaMemset(p, 0, sizeof(int));
-    words[dev] = p;
-  }
-  return words[dev];
 }
 
 }  // namespace
@@ -565,14 +575,11 @@ void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t
     }
 }
 
-// Rows [0, nblk * 512 * E) of every source and row, all 16-byte aligned.
-cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
-                          const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream) {
-  if (!nblk) return cudaSuccess;
+namespace {
+
+cudaError_t launch_common(Gf2Launch& a, int field, size_t k, size_t m, const uint32_t* bits, uint64_t nblk,
+                          bool overwrite, cudaStream_t stream) {
   const int E = field_bytes(field);
-  static thread_local Gf2Launch a;
-  for (size_t t = 0; t < k; ++t) a.src[t] = srcs[t];
-  for (size_t j = 0; j < m; ++j) a.dst[j] = rows[j];
   a.nblk = nblk;
   a.k = static_cast<uint32_t>(k);
   a.m = static_cast<uint32_t>(m);
@@ -580,8 +587,6 @@ cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8
   a.ngroups = static_cast<uint32_t>((k * E + 3) / 4);
   a.npad = static_cast<uint32_t>((m * E * 8 + 15) / 16 * 16);
   a.overwrite = overwrite ? 1u : 0u;
-  a.err = error_word();
-  if (!a.err) return cudaErrorMemoryAllocation;
   std::memcpy(a.bits, bits, sizeof a.bits);
   const uint32_t K = a.ngroups * 32u;
   const uint32_t b_bytes = (a.npad * K + 1023u) & ~1023u;
@@ -592,7 +597,7 @@ cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8
                                     : reinterpret_cast<const void*>(gf2mma_kernel<4>));
   // one CTA per SM: TMEM (512 columns) is allocated whole
   const int smem_launch = std::max(smem, 116 * 1024);
-  cudaError_t e = ensure_smem_attr(fn, smem_launch);
+  cudaError_t e = ensure_smem_attr(fn, kMaxLaunchSmem);
   if (e != cudaSuccess) return e;
   const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(nblk, static_cast<uint64_t>(sm_count())));
   if (E == 1)
@@ -604,13 +609,47 @@ cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8
   return cudaGetLastError();
 }
 
+}  // namespace
+
+cudaError_t gf2mma_prepare(int E) {
+  const void* fn = E == 1 ? reinterpret_cast<const void*>(gf2mma_kernel<1>)
+                          : (E == 2 ? reinterpret_cast<const void*>(gf2mma_kernel<2>)
+                                    : reinterpret_cast<const void*>(gf2mma_kernel<4>));
+  return ensure_smem_attr(fn, kMaxLaunchSmem);
+}
+
+// Rows [0, nblk * 512 * E) of every source and row, all 16-byte aligned.
+cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
+                          const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream) {
+  if (!nblk) return cudaSuccess;
+  static thread_local Gf2Launch a;
+  for (size_t t = 0; t < k; ++t) a.src[t] = srcs[t];
+  for (size_t j = 0; j < m; ++j) a.dst[j] = rows[j];
+  a.ptrs = a.prefix = nullptr;
+  a.nstripes = 0;
+  return launch_common(a, field, k, m, bits, nblk, overwrite, stream);
+}
+
+// Several stripes of one plan: ptrs / prefix are device arrays (see Gf2Launch).
+cudaError_t gf2mma_launch_multi(int field, size_t k, size_t m, const uint32_t* bits, const uint64_t* ptrs,
+                                const uint64_t* prefix, uint32_t nstripes, uint64_t nblk, bool overwrite,
+                                cudaStream_t stream) {
+  if (!nblk || !nstripes) return cudaSuccess;
+  static thread_local Gf2Launch a;
+  a.ptrs = ptrs;
+  a.prefix = prefix;
+  a.nstripes = nstripes;
+  return launch_common(a, field, k, m, bits, nblk, overwrite, stream);
+}
+
 // Error word of the current device: nonzero when a bounded wait ran out.
 int gf2mma_error(bool clear) {
-  int* p = error_word();
-  if (!p) return -1;
   int v = 0;
-  if (cudaMemcpy(&v, p, sizeof v, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-  if (clear && v) cudaMemset(p, 0, sizeof(int));
+  if (cudaMemcpyFromSymbol(&v, g_gf2_err, sizeof v) != cudaSuccess) return -1;
+  if (clear && v) {
+    const int zero = 0;
+    if (cudaMemcpyToSymbol(g_gf2_err, &zero, sizeof zero) != cudaSuccess) return -1;
+  }
   return v;
 }
 

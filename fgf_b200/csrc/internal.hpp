@@ -81,6 +81,14 @@ void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t
 // Columns [0, nblk * 512 * E) of k sources and m rows, all 16-byte aligned.
 cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
                           const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream);
+// Several stripes of one plan in one launch: ptrs (device) holds k source and
+// m row pointers per stripe, prefix (device) the first block of each stripe.
+cudaError_t gf2mma_launch_multi(int field, size_t k, size_t m, const uint32_t* bits, const uint64_t* ptrs,
+                                const uint64_t* prefix, uint32_t nstripes, uint64_t nblk, bool overwrite,
+                                cudaStream_t stream);
+// Opt the tensor-core kernel of element width E in to its shared memory on
+// the current device (done before a graph capture records a launch).
+cudaError_t gf2mma_prepare(int E);
 // Error word of the current device's tensor-core kernels (0 = fine);
 // synchronises with the device.
 int gf2mma_error(bool clear);
@@ -103,14 +111,30 @@ struct LoweredJob {
   std::vector<uint64_t> srcs, dsts;
 };
 
+// One stripe's 16-byte-aligned body for the tensor-core kernel in a batch:
+// its k sources and m rows already offset to the body start, nblk blocks of
+// 512 element columns.
+struct Gf2Job {
+  int field;
+  const uint32_t* bits;  // the plan's GF(2) bit matrix (host copy)
+  uint64_t bits_key;     // hash of the bit matrix: stripes with equal keys share a launch
+  size_t k, m;
+  bool ovr;
+  uint64_t nblk;
+  std::vector<uint64_t> ptrs;  // k sources, then m rows
+};
+
 void* batch_state_create();
 void batch_state_destroy(void* state);
 void batch_state_graphs(void* state, bool on);
 void batch_state_stats(const void* state, size_t* launches, size_t* items, int* replayed);
-cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, cudaStream_t stream);
-// One stripe of a plan (api.cpp) as sub-jobs for batch_run.
+cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const std::vector<Gf2Job>& tc,
+                      cudaStream_t stream);
+// One stripe of a plan (api.cpp) as sub-jobs for batch_run: the tensor-core
+// body (when the tuner picks that kernel for the shape and every pointer
+// shares one offset within 16 bytes) plus table sub-jobs for the rest.
 void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
-                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out);
+                      size_t row_len, bool overwrite, std::vector<LoweredJob>& out, std::vector<Gf2Job>& tc);
 
 // Error text of the calling thread (api.cpp), for entry points defined in
 // other files.

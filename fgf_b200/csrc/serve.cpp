@@ -437,6 +437,7 @@ void fgfc_server::issue(Launch* L) {
   // one submission of the work-list kernel for every request
   if (e == cudaSuccess) {
     std::vector<LoweredJob> low;
+    std::vector<Gf2Job> tc;
     std::vector<uint64_t> sp, dp;
     for (Req* r : L->reqs) {
       sp.resize(r->k);
@@ -445,9 +446,9 @@ void fgfc_server::issue(Launch* L) {
         sp[t] = reinterpret_cast<uint64_t>(r->on_device ? r->src[t] : dbase + r->d_src + t * r->Ls);
       for (size_t j = 0; j < r->m; ++j)
         dp[j] = reinterpret_cast<uint64_t>(r->on_device ? r->dst + r->starts[j] : dbase + r->d_rows + j * r->Ls);
-      lower_matrix_job(r->plan->plan, sp, dp, r->L, r->ovr, low);
+      lower_matrix_job(r->plan->plan, sp, dp, r->L, r->ovr, low, tc);
     }
-    e = batch_run(batch, low, s_run);
+    e = batch_run(batch, low, tc, s_run);
   }
   if (e == cudaSuccess) e = cudaEventRecord(L->ev_done, s_run);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(s_out, L->ev_done, 0);

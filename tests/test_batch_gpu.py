@@ -191,3 +191,68 @@ def test_batch_uniform_class_over_one_parameter_block(cuda):
         orc.dot_product_matrix(orc.GF8D, want, rl, m, coeffs,
                                [data[(s * k + t) * rl:(s * k + t + 1) * rl] for t in range(k)])
         assert np.array_equal(got[s * m * rl:(s + 1) * m * rl], want), s
+
+
+def test_tensor_core_bodies_in_a_batch(cuda):
+    """Stripes whose shape the tuner gives the tensor-core contraction run
+    their 16-byte-aligned bodies as one launch per plan (several stripes of
+    one plan share it) and their heads and tails on the table kernels. Every
+    byte against the oracle, in two submissions with fresh data."""
+    from fgf_b200 import tune
+
+    rng = np.random.default_rng(91)
+    specs = [  # field, k, m, row bytes, head offset, overwrite, scattered, plan id
+        (Gf16, 32, 8, 2 * 150000 + 6, 0, True, False, 0),
+        (Gf16, 32, 8, 2 * 131072, 0, True, False, 0),      # same plan: shares the launch
+        (Gf16, 5, 3, 2 * 140003, 4, False, False, 1),      # unaligned head, accumulate
+        (Gf8D, 10, 8, 300000 + 48, 0, True, True, 2),      # overwrite into scattered rows
+        (Gf8B, 64, 16, 262144 + 1000, 0, True, False, 3),
+        (Gf32, 16, 4, 4 * 70000, 8, True, False, 4),
+        (Gf32, 7, 3, 4 * 80000, 0, False, True, 5),        # accumulate into scattered rows
+    ]
+    plans = {}
+    for field, k, m, rl, hoff, ovr, sc, pid in specs:
+        assert tune.chosen(field, k, m, rl) == "gf2mma", (field.__name__, k, m, rl)
+        if pid not in plans:
+            coeffs = [int(x) for x in rng.integers(0, 1 << (8 * field.BYTES), size=k * m, dtype=np.uint64)]
+            plans[pid] = (coeffs, ops.Plan.matrix(field, k, m, coeffs))
+    b = fb.Batch(graphs=True)
+    for round_ in range(2):
+        jobs, checks = [], []
+        for field, k, m, rl, hoff, ovr, sc, pid in specs:
+            coeffs, plan = plans[pid]
+            stride = (rl + hoff + 64 + 255) // 256 * 256
+            src_pool = d(rng.integers(0, 256, size=k * stride, dtype=np.uint8))
+            srcs = [src_pool[t * stride + hoff:t * stride + hoff + rl] for t in range(k)]
+            if sc:
+                gap = (rl + 16 + 15) // 16 * 16 + 32
+                dst = d(rng.integers(0, 256, size=gap * m + hoff + 16, dtype=np.uint8))[hoff:hoff + gap * m]
+                starts = [j * gap for j in range(m)][::-1]
+            else:
+                dst = d(rng.integers(0, 256, size=rl * m + hoff + 16, dtype=np.uint8))[hoff:hoff + rl * m]
+                starts = None
+            want = h(dst).copy()
+            hs = [h(x).copy() for x in srcs]
+            if sc:
+                if ovr:
+                    for st in starts:
+                        want[st:st + rl] = 0
+                orc.mul_add_matrix_scattered(field.ID, want, rl, starts, coeffs, hs)
+            elif ovr:
+                orc.dot_product_matrix(field.ID, want, rl, m, coeffs, hs)
+            else:
+                orc.mul_add_matrix(field.ID, want, rl, m, coeffs, hs)
+            jobs.append(fb.Job(plan, srcs, dst, rl, m, ovr, starts))
+            checks.append((dst, want, srcs, src_pool))
+        b.run(jobs)
+        torch.cuda.synchronize()
+        assert _lib_device_ok()
+        for i, (dst, want, _, _) in enumerate(checks):
+            got = h(dst)
+            assert np.array_equal(got, want), f"round {round_}, stripe {i}: {int(np.count_nonzero(got != want))} bytes"
+
+
+def _lib_device_ok():
+    from fgf_b200 import _lib
+
+    return _lib.lib().fgfc_device_check(1) == 0
