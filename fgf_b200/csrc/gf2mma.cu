@@ -19,17 +19,20 @@
 // 2^23 (at most 512 products of 2^14), so the int32 accumulator is exact.
 //
 // Layout and flow of one CTA (one per SM, persistent over 512-column blocks):
-//   * warp 4 (producer): stages the k source rows of a block (512 columns,
+//   * the producer warp stages the k source rows of a block (512 columns,
 //     512 * E bytes per source) into a 4-deep shared-memory ring with
 //     cp.async.bulk (single GPU, no multicast), completion on an mbarrier;
-//   * warps 0..3 (workers, thread i owns TMEM lane i): read the 4 consecutive
-//     columns 4i..4i+3 of every source of a block into registers, then for
-//     each of the block's 4 tiles (tile q = columns 4i + q) build the A lane
-//     (K/4 32-bit TMEM columns) and write it with tcgen05.st; after a tile's
-//     product is done they read D back (tcgen05.ld), gather bit 7 of every
-//     accumulator into output bytes with PRMT and two multiply-adds, and
-//     after the 4th tile store 4 consecutive columns of every row;
-//   * warp 5 (issuer): allocates TMEM (A and D double-buffered, 512 columns),
+//   * warps 0..15 (workers; thread i of a lane quarter owns TMEM lane i, and
+//     the 4 warps of a quarter split the work of every tile): read the 4
+//     consecutive columns 4i..4i+3 of their share of the sources into
+//     registers, then for each of the block's 4 tiles (tile q = columns
+//     4i + q) build their part of the A lane and write it with tcgen05.st;
+//     after a tile's product is done they read their part of D back
+//     (tcgen05.ld), gather bit 7 of every accumulator into output bytes with
+//     PRMT and two multiply-adds, and after the 4th tile store 4 consecutive
+//     columns of their rows;
+//   * warp 16 (producer): see above, every lane issuing copies;
+//   * warp 17 (issuer): allocates TMEM (A and D double-buffered, 512 columns),
 //     issues K/32 tcgen05.mma per tile from one thread and commits each tile
 //     to an mbarrier.
 // Every mbarrier wait is bounded: a wait that runs out sets the error word,
@@ -50,7 +53,11 @@ namespace fgfc {
 
 namespace {
 
-constexpr int kMmaThreads = 192;       // 4 worker warps, producer, issuer
+constexpr int kParts = 4;                              // worker warps per TMEM lane quarter
+constexpr int kWorkerWarps = 4 * kParts;               // warps 0 .. 15
+constexpr int kProducerWarp = kWorkerWarps;            // bulk copies of source blocks
+constexpr int kIssuerWarp = kWorkerWarps + 1;          // TMEM allocation and the products
+constexpr int kMmaThreads = (kWorkerWarps + 2) * 32;   // 576
 constexpr int kStages = 4;
 constexpr uint32_t kCols = 512;        // element columns per block (4 tiles of 128)
 constexpr uint32_t kMaxInBits = 512;   // K
@@ -243,113 +250,128 @@ struct Smem {
   int abort;
 };
 
-// Epilogue of tile tt (columns 4i + q of its block, q = tt % 4, TMEM buffer
-// tt % 2): read the accumulators, fold bit 7 of each into output byte v of
-// column q (byte q of out[v]); after the 4th tile store 4 columns of every row.
+// Worker warps come in 4 parts per TMEM lane quarter: warp w owns TMEM lanes
+// 32 (w % 4) .. + 31 (element columns of a tile) and part p = w / 4 of the
+// work of every tile: input groups 4p .. 4p + 3 (input bytes 16p .. 16p + 15)
+// and output bytes 4p .. 4p + 3 (D columns 32p .. 32p + 31). So each warp
+// issues one 32-column TMEM store and one 32-column TMEM load per tile, and
+// every SM scheduler holds 4 worker warps to hide their latencies.
+
+// Epilogue of tile tt (columns 4i + Q of its block, TMEM buffer Q % 2): read
+// this part's accumulators, fold bit 7 of each into output byte 4p + v of
+// column Q (byte Q of out[v]); after the 4th tile store 4 columns of this
+// part's rows.
 template <int E, int Q>
 __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
-                                         uint32_t (&out)[16], volatile int* abort, StripeCursor& cur) {
+                                         uint32_t (&out)[4], volatile int* abort, StripeCursor& cur) {
   constexpr uint32_t b = Q & 1;
   constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
-  const uint32_t warp = threadIdx.x >> 5, i = threadIdx.x;
-  const uint32_t lane_base = (warp * 32u) << 16;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t part = warp >> 2, i = (warp & 3u) * 32u + lane;
+  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
   if (!warp_wait(&S.dfull[b], static_cast<uint32_t>((tt >> 1) & 1u), abort)) return false;
   tc_fence_after();
+  const uint32_t c0 = 32u * part;
+  if (c0 >= a.npad) return true;  // no output bytes in this part (warp-uniform)
+  uint32_t r[32];
+  if (a.npad - c0 >= 32) {
+    tmem_ld32(lane_base | (d_col[b] + c0), r);
+  } else {
+    tmem_ld16(lane_base | (d_col[b] + c0), r);
+#pragma unroll
+    for (int x = 16; x < 32; ++x) r[x] = 0;
+  }
+  tmem_wait_ld();
   const uint32_t nout = a.m * E;
 #pragma unroll
-  for (uint32_t c = 0; c < kMaxOutBits / 32; ++c) {
-    const uint32_t c0 = 32u * c;
-    if (c0 >= a.npad) break;
-    uint32_t r[32];
-    if (a.npad - c0 >= 32) {
-      tmem_ld32(lane_base | (d_col[b] + c0), r);
-    } else {
-      tmem_ld16(lane_base | (d_col[b] + c0), r);
-#pragma unroll
-      for (int x = 16; x < 32; ++x) r[x] = 0;
-    }
-    tmem_wait_ld();
-#pragma unroll
-    for (uint32_t v = 0; v < 4; ++v)
-      if (4 * c + v < nout) out[4 * c + v] = prmt(out[4 * c + v], pack_byte(&r[8 * v]), qsel);
-  }
+  for (uint32_t v = 0; v < 4; ++v)
+    if (4 * part + v < nout) out[v] = prmt(out[v], pack_byte(&r[8 * v]), qsel);
   if (Q == 3) {
     const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
     const uint64_t off = static_cast<uint64_t>(i) * 4u * E;
+    if (E == 1) {  // rows 4p .. 4p + 3
 #pragma unroll
-    for (uint32_t j = 0; j < 16 / E; ++j) {
-      if (j >= a.m) break;
-      uint8_t* p = cur.at<E>(a, blk, a.k + j) + off;
-      if (E == 1) {
-        uint32_t v = out[j];
-        if (!a.overwrite) v ^= *reinterpret_cast<const uint32_t*>(p);
-        *reinterpret_cast<uint32_t*>(p) = v;
-      } else if (E == 2) {
-        uint2 v = make_uint2(prmt(out[2 * j], out[2 * j + 1], 0x5140u), prmt(out[2 * j], out[2 * j + 1], 0x7362u));
+      for (uint32_t jj = 0; jj < 4; ++jj) {
+        const uint32_t j = 4 * part + jj;
+        if (j >= a.m) break;
+        uint32_t* p = reinterpret_cast<uint32_t*>(cur.at<E>(a, blk, a.k + j) + off);
+        *p = a.overwrite ? out[jj] : (out[jj] ^ *p);
+      }
+    } else if (E == 2) {  // rows 2p, 2p + 1: bytes 0 and 1 of 4 elements, interleaved
+#pragma unroll
+      for (uint32_t jj = 0; jj < 2; ++jj) {
+        const uint32_t j = 2 * part + jj;
+        if (j >= a.m) break;
+        uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + off);
+        uint2 v = make_uint2(prmt(out[2 * jj], out[2 * jj + 1], 0x5140u), prmt(out[2 * jj], out[2 * jj + 1], 0x7362u));
         if (!a.overwrite) {
-          const uint2 d = *reinterpret_cast<const uint2*>(p);
+          const uint2 d = *p;
           v.x ^= d.x;
           v.y ^= d.y;
         }
-        *reinterpret_cast<uint2*>(p) = v;
-      } else {
-        uint4 v = make_uint4(row_word4(&out[4 * j], 0), row_word4(&out[4 * j], 1), row_word4(&out[4 * j], 2),
-                             row_word4(&out[4 * j], 3));
+        *p = v;
+      }
+    } else {  // row p: 4 bytes of 4 elements, transposed
+      const uint32_t j = part;
+      if (j < a.m) {
+        uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + off);
+        uint4 v = make_uint4(row_word4(out, 0), row_word4(out, 1), row_word4(out, 2), row_word4(out, 3));
         if (!a.overwrite) {
-          const uint4 d = *reinterpret_cast<const uint4*>(p);
+          const uint4 d = *p;
           v.x ^= d.x;
           v.y ^= d.y;
           v.z ^= d.z;
           v.w ^= d.w;
         }
-        *reinterpret_cast<uint4*>(p) = v;
+        *p = v;
       }
     }
   }
   return true;
 }
 
-// The A lane of tile Q (column 4i + Q of the block) into TMEM buffer Q % 2.
-// Group g = input bytes 4g..4g+3 of the column (input byte u = t * E + p);
-// TMEM column 8g + b holds bit b of those 4 bytes, each as the value 2^b.
+// This part's groups of the A lane of tile Q (column 4i + Q of the block)
+// into TMEM buffer Q % 2. Group g = input bytes 4g..4g+3 of the column (input
+// byte u = t * E + p); TMEM column 8g + b holds bit b of those 4 bytes, each
+// as the value 2^b. sw holds this thread's words of input bytes 16p ..
+// 16p + 15 (global word 16p + x is sw[x]).
 template <int E, int Q>
-__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[64], uint32_t a_col) {
+__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[16], uint32_t a_col) {
   const uint32_t warp = threadIdx.x >> 5;
-  const uint32_t lane_base = (warp * 32u) << 16;
+  const uint32_t part = warp >> 2;
+  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+  const uint32_t g0 = 4u * part;
+  if (g0 >= a.ngroups) return;  // warp-uniform
   const uint32_t nwords = a.k * E;
+  uint32_t col[32];
 #pragma unroll
-  for (uint32_t g0 = 0; g0 < 16; g0 += 4) {
-    if (g0 >= a.ngroups) break;
-    uint32_t col[32];
-#pragma unroll
-    for (uint32_t gg = 0; gg < 4; ++gg) {
-      const uint32_t g = g0 + gg;
-      uint32_t wg;
-      if (E == 1) {  // sources 4g..4g+3, byte Q of each
-        constexpr uint32_t qs = Q | ((4u + Q) << 4);
-        const uint32_t s0 = 4 * g < nwords ? sw[4 * g] : 0u;
-        const uint32_t s1 = 4 * g + 1 < nwords ? sw[4 * g + 1] : 0u;
-        const uint32_t s2 = 4 * g + 2 < nwords ? sw[4 * g + 2] : 0u;
-        const uint32_t s3 = 4 * g + 3 < nwords ? sw[4 * g + 3] : 0u;
-        wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
-      } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
-        const uint32_t x0 = 4 * g + Q / 2 < nwords ? sw[4 * g + Q / 2] : 0u;
-        const uint32_t x1 = 4 * g + 2 + Q / 2 < nwords ? sw[4 * g + 2 + Q / 2] : 0u;
-        wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
-      } else {  // source g, element Q
-        wg = 4 * g + Q < nwords ? sw[4 * g + Q] : 0u;
-      }
-#pragma unroll
-      for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
+  for (uint32_t gg = 0; gg < 4; ++gg) {
+    const uint32_t gw = 16u * part + 4u * gg;  // global word of the group's first input byte
+    uint32_t wg;
+    if (E == 1) {  // sources 4g..4g+3, byte Q of each
+      constexpr uint32_t qs = Q | ((4u + Q) << 4);
+      const uint32_t s0 = gw < nwords ? sw[4 * gg] : 0u;
+      const uint32_t s1 = gw + 1 < nwords ? sw[4 * gg + 1] : 0u;
+      const uint32_t s2 = gw + 2 < nwords ? sw[4 * gg + 2] : 0u;
+      const uint32_t s3 = gw + 3 < nwords ? sw[4 * gg + 3] : 0u;
+      wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
+    } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
+      const uint32_t x0 = gw + Q / 2 < nwords ? sw[4 * gg + Q / 2] : 0u;
+      const uint32_t x1 = gw + 2 + Q / 2 < nwords ? sw[4 * gg + 2 + Q / 2] : 0u;
+      wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
+    } else {  // source g, element Q
+      wg = gw + Q < nwords ? sw[4 * gg + Q] : 0u;
     }
-    const uint32_t taddr = lane_base | (a_col + 8u * g0);
-    if (a.ngroups - g0 >= 4) {
-      tmem_st32(taddr, col);
-    } else {
 #pragma unroll
-      for (uint32_t gg = 0; gg < 3; ++gg)
-        if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
-    }
+    for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
+  }
+  const uint32_t taddr = lane_base | (a_col + 8u * g0);
+  if (a.ngroups - g0 >= 4) {
+    tmem_st32(taddr, col);
+  } else {
+#pragma unroll
+    for (uint32_t gg = 0; gg < 3; ++gg)
+      if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
   }
   tmem_wait_st();
 }
@@ -358,11 +380,14 @@ template <int E>
 __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
                                             uint64_t nmine, const uint32_t (&a_col)[2], const uint32_t (&d_col)[2],
                                             volatile int* abort) {
-  const uint32_t lane = threadIdx.x & 31u, i = threadIdx.x;
-  uint32_t sw[64];   // this thread's 4 columns of every source (k * E words)
-  uint32_t out[16];  // output byte v of the 4 columns
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t part = warp >> 2, i = (warp & 3u) * 32u + lane;
+  uint32_t sw[16];  // this thread's 4 columns of input bytes 16p .. 16p + 15
+  uint32_t out[4];  // output bytes 4p .. 4p + 3 of the 4 columns
 #pragma unroll
-  for (int x = 0; x < 16; ++x) out[x] = 0;
+  for (int x = 0; x < 4; ++x) out[x] = 0;
+#pragma unroll
+  for (int x = 0; x < 16; ++x) sw[x] = 0;
   const uint32_t nwords = a.k * E;
   bool ok = true;
   StripeCursor cur;
@@ -375,9 +400,10 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     }
     const uint8_t* st = stages + s * stage_bytes;
 #pragma unroll
-    for (uint32_t w = 0; w < 64; w += E) {
-      if (w >= nwords) break;
-      const uint8_t* p = st + (w / E) * kCols * E + i * 4u * E;
+    for (uint32_t w = 0; w < 16; w += E) {
+      const uint32_t gw = 16u * part + w;
+      if (gw >= nwords) break;
+      const uint8_t* p = st + (gw / E) * kCols * E + i * 4u * E;
       if (E == 1) {
         sw[w] = *reinterpret_cast<const uint32_t*>(p);
       } else if (E == 2) {
@@ -418,7 +444,6 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     atomicExch(&g_gf2_err, 3);
     *abort = 1;
   }
-  (void)nwords;
 }
 
 template <int E>
@@ -457,10 +482,10 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&S.full[s], 1);
-      mbar_init(&S.empty[s], 4);
+      mbar_init(&S.empty[s], kWorkerWarps);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&S.afull[b], 4);
+      mbar_init(&S.afull[b], kWorkerWarps);
       mbar_init(&S.dfull[b], 1);
     }
     S.abort = 0;
@@ -468,7 +493,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   }
   // generic-proxy writes of the B image become visible to the tensor cores
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  if (warp == 5) {
+  if (warp == kIssuerWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
                  "r"(kTmemCols)
                  : "memory");
@@ -485,30 +510,35 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   const uint64_t nmine = a.nblk > blockIdx.x ? (a.nblk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
   const uint64_t ntiles = nmine * 4u;
 
-  if (warp == 4) {
-    // ---- producer
+  if (warp == kProducerWarp) {
+    // ---- producer: lane 0 arms the stage's barrier, every lane issues copies
+    const uint32_t row_bytes = kCols * E;
+    StripeCursor cur;
     uint64_t issued = 0;
-    if (lane == 0) {
-      const uint32_t row_bytes = kCols * E;
-      StripeCursor cur;
-      for (uint64_t i = 0; i < nmine && !*abort; ++i) {
-        const uint32_t s = static_cast<uint32_t>(i % kStages);
-        if (i >= kStages && !mbar_wait(&S.empty[s], static_cast<uint32_t>((i / kStages - 1) & 1u), abort)) {
+    for (uint64_t i = 0; i < nmine; ++i) {
+      const uint32_t s = static_cast<uint32_t>(i % kStages);
+      int go = 1;
+      if (lane == 0) {
+        go = !*abort;
+        if (go && i >= kStages && !mbar_wait(&S.empty[s], static_cast<uint32_t>((i / kStages - 1) & 1u), abort)) {
           atomicExch(&g_gf2_err, 1);
           *abort = 1;
-          break;
+          go = 0;
         }
-        const uint64_t blk = blockIdx.x + i * gridDim.x;
-        mbar_expect_tx(&S.full[s], a.k * row_bytes);
-        for (uint32_t t = 0; t < a.k; ++t)
-          bulk_g2s(stages + s * stage_bytes + t * row_bytes, cur.at<E>(a, blk, t), row_bytes, &S.full[s]);
-        ++issued;
+        if (go) mbar_expect_tx(&S.full[s], a.k * row_bytes);
       }
-      // copies still in flight must land before the CTA exits
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
+      const uint64_t blk = blockIdx.x + i * gridDim.x;
+      for (uint32_t t = lane; t < a.k; t += 32)
+        bulk_g2s(stages + s * stage_bytes + t * row_bytes, cur.at<E>(a, blk, t), row_bytes, &S.full[s]);
+      ++issued;
+    }
+    // copies still in flight must land before the CTA exits
+    if (lane == 0)
       for (uint64_t i = issued > kStages ? issued - kStages : 0; i < issued; ++i)
         mbar_wait(&S.full[i % kStages], static_cast<uint32_t>((i / kStages) & 1u), abort, false);
-    }
-  } else if (warp == 5) {
+  } else if (warp == kIssuerWarp) {
     // ---- issuer: one thread issues every product of a tile
     if (lane == 0) {
       const uint32_t idesc = (2u << 4) | ((a.npad >> 3) << 17) | ((128u >> 4) << 24);  // s32 += u8 * u8, M = 128
@@ -532,13 +562,13 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
         mbar_wait(&S.dfull[u & 1u], static_cast<uint32_t>((u >> 1) & 1u), abort, false);
     }
   } else {
-    // ---- workers: thread i owns TMEM lane i and columns 4i..4i+3 of a block
+    // ---- workers
     worker_loop<E>(a, S, stages, stage_bytes, nmine, a_col, d_col, abort);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 5)
+  if (warp == kIssuerWarp)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
 }
 
