@@ -22,15 +22,14 @@
 //   * the producer warp stages the k source rows of a block (512 columns,
 //     512 * E bytes per source) into a 4-deep shared-memory ring with
 //     cp.async.bulk (single GPU, no multicast), completion on an mbarrier;
-//   * warps 0..15 (workers; thread i of a lane quarter owns TMEM lane i, and
-//     the 4 warps of a quarter split the work of every tile): read the 4
-//     consecutive columns 4i..4i+3 of their share of the sources into
-//     registers, then for each of the block's 4 tiles (tile q = columns
-//     4i + q) build their part of the A lane and write it with tcgen05.st;
-//     after a tile's product is done they read their part of D back
-//     (tcgen05.ld), gather bit 7 of every accumulator into output bytes with
-//     PRMT and two multiply-adds, and after the 4th tile store 4 consecutive
-//     columns of their rows;
+//   * warps 0..7 (expanders; thread i of a lane quarter owns TMEM lane i):
+//     read the 4 consecutive columns 4i..4i+3 of their half of the sources
+//     into registers, then for each of the block's 4 tiles (tile q = columns
+//     4i + q) build their half of the A lane and write it with tcgen05.st;
+//   * warps 8..15 (epilogue): when a tile's product is done, read their half
+//     of D back (tcgen05.ld), release the buffer, gather bit 7 of every
+//     accumulator into output bytes with PRMT and two multiply-adds, and
+//     after the 4th tile store 4 consecutive columns of their rows;
 //   * warp 16 (producer): see above, every lane issuing copies;
 //   * warp 17 (issuer): allocates TMEM (A and D double-buffered, 512 columns),
 //     issues K/32 tcgen05.mma per tile from one thread and commits each tile
@@ -53,8 +52,8 @@ namespace fgfc {
 
 namespace {
 
-constexpr int kParts = 4;                              // worker warps per TMEM lane quarter
-constexpr int kWorkerWarps = 4 * kParts;               // warps 0 .. 15
+constexpr int kExpandWarps = 8;                        // warps 0 .. 7: write A lanes
+constexpr int kWorkerWarps = 16;                       // + warps 8 .. 15: read D back
 constexpr int kProducerWarp = kWorkerWarps;            // bulk copies of source blocks
 constexpr int kIssuerWarp = kWorkerWarps + 1;          // TMEM allocation and the products
 constexpr int kMmaThreads = (kWorkerWarps + 2) * 32;   // 576
@@ -245,152 +244,79 @@ __device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
 }
 
 struct Smem {
-  uint64_t full[kStages], empty[kStages], afull[2], dfull[2];
+  uint64_t full[kStages], empty[kStages], afull[2], dfull[2], dempty[2];
   uint32_t tmem_base;
   int abort;
 };
 
-// Worker warps come in 4 parts per TMEM lane quarter: warp w owns TMEM lanes
-// 32 (w % 4) .. + 31 (element columns of a tile) and part p = w / 4 of the
-// work of every tile: input groups 4p .. 4p + 3 (input bytes 16p .. 16p + 15)
-// and output bytes 4p .. 4p + 3 (D columns 32p .. 32p + 31). So each warp
-// issues one 32-column TMEM store and one 32-column TMEM load per tile, and
-// every SM scheduler holds 4 worker warps to hide their latencies.
+// The 16 worker warps have two jobs. Expander warp e (0..7) and epilogue warp
+// e (8..15) own TMEM lanes 32 (e % 4) .. + 31, the element columns of a tile,
+// and half h = (e % 8) / 4 of their job: an expander writes input groups
+// 8h .. 8h + 7 of the A lanes (input bytes 32h .. 32h + 31), an epilogue warp
+// reads output bytes 8h .. 8h + 7 (D columns 64h .. 64h + 63). Expanders
+// refill A for tile t as soon as the product of tile t - 2 has finished
+// with it, while epilogue warps read that product back, so the chain between
+// two products is the longer of the two jobs, not their sum.
 
-// Epilogue of tile tt (columns 4i + Q of its block, TMEM buffer Q % 2): read
-// this part's accumulators, fold bit 7 of each into output byte 4p + v of
-// column Q (byte Q of out[v]); after the 4th tile store 4 columns of this
-// part's rows.
-template <int E, int Q>
-__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
-                                         uint32_t (&out)[4], volatile int* abort, StripeCursor& cur) {
-  constexpr uint32_t b = Q & 1;
-  constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t part = warp >> 2, i = (warp & 3u) * 32u + lane;
-  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  if (!warp_wait(&S.dfull[b], static_cast<uint32_t>((tt >> 1) & 1u), abort)) return false;
-  tc_fence_after();
-  const uint32_t c0 = 32u * part;
-  if (c0 >= a.npad) return true;  // no output bytes in this part (warp-uniform)
-  uint32_t r[32];
-  if (a.npad - c0 >= 32) {
-    tmem_ld32(lane_base | (d_col[b] + c0), r);
-  } else {
-    tmem_ld16(lane_base | (d_col[b] + c0), r);
-#pragma unroll
-    for (int x = 16; x < 32; ++x) r[x] = 0;
-  }
-  tmem_wait_ld();
-  const uint32_t nout = a.m * E;
-#pragma unroll
-  for (uint32_t v = 0; v < 4; ++v)
-    if (4 * part + v < nout) out[v] = prmt(out[v], pack_byte(&r[8 * v]), qsel);
-  if (Q == 3) {
-    const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
-    const uint64_t off = static_cast<uint64_t>(i) * 4u * E;
-    if (E == 1) {  // rows 4p .. 4p + 3
-#pragma unroll
-      for (uint32_t jj = 0; jj < 4; ++jj) {
-        const uint32_t j = 4 * part + jj;
-        if (j >= a.m) break;
-        uint32_t* p = reinterpret_cast<uint32_t*>(cur.at<E>(a, blk, a.k + j) + off);
-        *p = a.overwrite ? out[jj] : (out[jj] ^ *p);
-      }
-    } else if (E == 2) {  // rows 2p, 2p + 1: bytes 0 and 1 of 4 elements, interleaved
-#pragma unroll
-      for (uint32_t jj = 0; jj < 2; ++jj) {
-        const uint32_t j = 2 * part + jj;
-        if (j >= a.m) break;
-        uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + off);
-        uint2 v = make_uint2(prmt(out[2 * jj], out[2 * jj + 1], 0x5140u), prmt(out[2 * jj], out[2 * jj + 1], 0x7362u));
-        if (!a.overwrite) {
-          const uint2 d = *p;
-          v.x ^= d.x;
-          v.y ^= d.y;
-        }
-        *p = v;
-      }
-    } else {  // row p: 4 bytes of 4 elements, transposed
-      const uint32_t j = part;
-      if (j < a.m) {
-        uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + off);
-        uint4 v = make_uint4(row_word4(out, 0), row_word4(out, 1), row_word4(out, 2), row_word4(out, 3));
-        if (!a.overwrite) {
-          const uint4 d = *p;
-          v.x ^= d.x;
-          v.y ^= d.y;
-          v.z ^= d.z;
-          v.w ^= d.w;
-        }
-        *p = v;
-      }
-    }
-  }
-  return true;
-}
-
-// This part's groups of the A lane of tile Q (column 4i + Q of the block)
+// This half's groups of the A lane of tile Q (column 4i + Q of the block)
 // into TMEM buffer Q % 2. Group g = input bytes 4g..4g+3 of the column (input
 // byte u = t * E + p); TMEM column 8g + b holds bit b of those 4 bytes, each
-// as the value 2^b. sw holds this thread's words of input bytes 16p ..
-// 16p + 15 (global word 16p + x is sw[x]).
+// as the value 2^b. sw holds this thread's words of input bytes 32h .. 32h +
+// 31 (global word 32h + x is sw[x]).
 template <int E, int Q>
-__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[16], uint32_t a_col) {
-  const uint32_t warp = threadIdx.x >> 5;
-  const uint32_t part = warp >> 2;
-  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  const uint32_t g0 = 4u * part;
-  if (g0 >= a.ngroups) return;  // warp-uniform
+__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[32], uint32_t a_col, uint32_t half,
+                                       uint32_t lane_base) {
   const uint32_t nwords = a.k * E;
-  uint32_t col[32];
 #pragma unroll
-  for (uint32_t gg = 0; gg < 4; ++gg) {
-    const uint32_t gw = 16u * part + 4u * gg;  // global word of the group's first input byte
-    uint32_t wg;
-    if (E == 1) {  // sources 4g..4g+3, byte Q of each
-      constexpr uint32_t qs = Q | ((4u + Q) << 4);
-      const uint32_t s0 = gw < nwords ? sw[4 * gg] : 0u;
-      const uint32_t s1 = gw + 1 < nwords ? sw[4 * gg + 1] : 0u;
-      const uint32_t s2 = gw + 2 < nwords ? sw[4 * gg + 2] : 0u;
-      const uint32_t s3 = gw + 3 < nwords ? sw[4 * gg + 3] : 0u;
-      wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
-    } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
-      const uint32_t x0 = gw + Q / 2 < nwords ? sw[4 * gg + Q / 2] : 0u;
-      const uint32_t x1 = gw + 2 + Q / 2 < nwords ? sw[4 * gg + 2 + Q / 2] : 0u;
-      wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
-    } else {  // source g, element Q
-      wg = gw + Q < nwords ? sw[4 * gg + Q] : 0u;
+  for (uint32_t c = 0; c < 2; ++c) {
+    const uint32_t g0 = 8u * half + 4u * c;
+    if (g0 >= a.ngroups) break;  // warp-uniform
+    uint32_t col[32];
+#pragma unroll
+    for (uint32_t gg = 0; gg < 4; ++gg) {
+      const uint32_t lw = 16u * c + 4u * gg;        // local word of the group's first input byte
+      const uint32_t gw = 32u * half + lw;          // global word
+      uint32_t wg;
+      if (E == 1) {  // sources 4g..4g+3, byte Q of each
+        constexpr uint32_t qs = Q | ((4u + Q) << 4);
+        const uint32_t s0 = gw < nwords ? sw[lw] : 0u;
+        const uint32_t s1 = gw + 1 < nwords ? sw[lw + 1] : 0u;
+        const uint32_t s2 = gw + 2 < nwords ? sw[lw + 2] : 0u;
+        const uint32_t s3 = gw + 3 < nwords ? sw[lw + 3] : 0u;
+        wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
+      } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
+        const uint32_t x0 = gw + Q / 2 < nwords ? sw[lw + Q / 2] : 0u;
+        const uint32_t x1 = gw + 2 + Q / 2 < nwords ? sw[lw + 2 + Q / 2] : 0u;
+        wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
+      } else {  // source g, element Q
+        wg = gw + Q < nwords ? sw[lw + Q] : 0u;
+      }
+#pragma unroll
+      for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
     }
+    const uint32_t taddr = lane_base | (a_col + 8u * g0);
+    if (a.ngroups - g0 >= 4) {
+      tmem_st32(taddr, col);
+    } else {
 #pragma unroll
-    for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
-  }
-  const uint32_t taddr = lane_base | (a_col + 8u * g0);
-  if (a.ngroups - g0 >= 4) {
-    tmem_st32(taddr, col);
-  } else {
-#pragma unroll
-    for (uint32_t gg = 0; gg < 3; ++gg)
-      if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
+      for (uint32_t gg = 0; gg < 3; ++gg)
+        if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
+    }
   }
   tmem_wait_st();
 }
 
 template <int E>
-__device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
-                                            uint64_t nmine, const uint32_t (&a_col)[2], const uint32_t (&d_col)[2],
-                                            volatile int* abort) {
+__device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
+                                              uint64_t nmine, const uint32_t (&a_col)[2], volatile int* abort) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t part = warp >> 2, i = (warp & 3u) * 32u + lane;
-  uint32_t sw[16];  // this thread's 4 columns of input bytes 16p .. 16p + 15
-  uint32_t out[4];  // output bytes 4p .. 4p + 3 of the 4 columns
+  const uint32_t half = warp >> 2, i = (warp & 3u) * 32u + lane;
+  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+  uint32_t sw[32];  // this thread's 4 columns of input bytes 32h .. 32h + 31
 #pragma unroll
-  for (int x = 0; x < 4; ++x) out[x] = 0;
-#pragma unroll
-  for (int x = 0; x < 16; ++x) sw[x] = 0;
+  for (int x = 0; x < 32; ++x) sw[x] = 0;
   const uint32_t nwords = a.k * E;
   bool ok = true;
-  StripeCursor cur;
   uint64_t t = 0;  // tiles expanded so far
   for (uint64_t it = 0; it < nmine && ok; ++it) {
     const uint32_t s = static_cast<uint32_t>(it % kStages);
@@ -400,8 +326,8 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     }
     const uint8_t* st = stages + s * stage_bytes;
 #pragma unroll
-    for (uint32_t w = 0; w < 16; w += E) {
-      const uint32_t gw = 16u * part + w;
+    for (uint32_t w = 0; w < 32; w += E) {
+      const uint32_t gw = 32u * half + w;
       if (gw >= nwords) break;
       const uint8_t* p = st + (gw / E) * kCols * E + i * 4u * E;
       if (E == 1) {
@@ -420,28 +346,133 @@ __device__ __forceinline__ void worker_loop(const Gf2Launch& a, Smem& S, const u
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.empty[s]);  // the stage may be refilled
-    // tile Q of this block is tile t + Q; before it reuses buffer Q % 2, the
-    // tile two before it (t + Q - 2) is read back
-#define FGFC_TILE(Q, PQ)                                                      \
-    if (ok && t + Q >= 2) ok = epilogue<E, PQ>(a, S, d_col, t + Q - 2, out, abort, cur); \
-    if (ok) {                                                                 \
-      expand<E, Q>(a, sw, a_col[Q & 1]);                                      \
-      tc_fence_before();                                                      \
-      __syncwarp();                                                           \
-      if (lane == 0) mbar_arrive(&S.afull[Q & 1]);                            \
+    // tile Q of this block is tile t + Q: buffer Q % 2 is free once the
+    // product of tile t + Q - 2 has finished
+#define FGFC_TILE(Q)                                                                          \
+    if (ok && t + Q >= 2)                                                                     \
+      ok = warp_wait(&S.dfull[Q & 1], static_cast<uint32_t>(((t + Q - 2) >> 1) & 1u), abort); \
+    if (ok) {                                                                                 \
+      tc_fence_after();                                                                       \
+      expand<E, Q>(a, sw, a_col[Q & 1], half, lane_base);                                     \
+      tc_fence_before();                                                                      \
+      __syncwarp();                                                                           \
+      if (lane == 0) mbar_arrive(&S.afull[Q & 1]);                                            \
     }
-    FGFC_TILE(0, 2)
-    FGFC_TILE(1, 3)
-    FGFC_TILE(2, 0)
-    FGFC_TILE(3, 1)
+    FGFC_TILE(0)
+    FGFC_TILE(1)
+    FGFC_TILE(2)
+    FGFC_TILE(3)
 #undef FGFC_TILE
     t += 4;
   }
-  // the last two tiles (columns 2 and 3 of the last block)
-  if (ok && t >= 2) ok = epilogue<E, 2>(a, S, d_col, t - 2, out, abort, cur);
-  if (ok && t >= 2) ok = epilogue<E, 3>(a, S, d_col, t - 1, out, abort, cur);
   if (!ok) {
     atomicExch(&g_gf2_err, 3);
+    *abort = 1;
+  }
+}
+
+// Epilogue of tile tt (columns 4i + Q of its block, TMEM buffer Q % 2): read
+// this half's accumulators and release the buffer, fold bit 7 of each into
+// output byte 8h + v of column Q (byte Q of out[v]); after the 4th tile
+// store 4 columns of this half's rows.
+template <int E, int Q>
+__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
+                                         uint32_t (&out)[8], volatile int* abort, StripeCursor& cur) {
+  constexpr uint32_t b = Q & 1;
+  constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t half = (warp >> 2) & 1u, i = (warp & 3u) * 32u + lane;
+  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+  if (!warp_wait(&S.dfull[b], static_cast<uint32_t>((tt >> 1) & 1u), abort)) return false;
+  tc_fence_after();
+  const uint32_t c0 = 64u * half;
+  const uint32_t nout = a.m * E;
+  // two 32-column loads, one at a time (registers), then the buffer is released
+#pragma unroll
+  for (uint32_t c = 0; c < 2; ++c) {
+    const uint32_t cc = c0 + 32u * c;
+    if (cc < a.npad) {  // warp-uniform
+      uint32_t r[32];
+      if (a.npad - cc >= 32) {
+        tmem_ld32(lane_base | (d_col[b] + cc), r);
+      } else {
+        tmem_ld16(lane_base | (d_col[b] + cc), r);
+#pragma unroll
+        for (int x = 16; x < 32; ++x) r[x] = 0;
+      }
+      tmem_wait_ld();
+#pragma unroll
+      for (uint32_t v = 0; v < 4; ++v)
+        if (8 * half + 4 * c + v < nout) out[4 * c + v] = prmt(out[4 * c + v], pack_byte(&r[8 * v]), qsel);
+    }
+  }
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&S.dempty[b]);  // the next product may overwrite D
+  if (c0 >= a.npad) return true;
+  if (Q == 3) {
+    const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
+    const uint64_t off = static_cast<uint64_t>(i) * 4u * E;
+    if (E == 1) {  // rows 8h .. 8h + 7
+#pragma unroll
+      for (uint32_t jj = 0; jj < 8; ++jj) {
+        const uint32_t j = 8 * half + jj;
+        if (j >= a.m) break;
+        uint32_t* p = reinterpret_cast<uint32_t*>(cur.at<E>(a, blk, a.k + j) + off);
+        *p = a.overwrite ? out[jj] : (out[jj] ^ *p);
+      }
+    } else if (E == 2) {  // rows 4h .. 4h + 3: bytes 0 and 1 of 4 elements, interleaved
+#pragma unroll
+      for (uint32_t jj = 0; jj < 4; ++jj) {
+        const uint32_t j = 4 * half + jj;
+        if (j >= a.m) break;
+        uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + off);
+        uint2 v = make_uint2(prmt(out[2 * jj], out[2 * jj + 1], 0x5140u), prmt(out[2 * jj], out[2 * jj + 1], 0x7362u));
+        if (!a.overwrite) {
+          const uint2 d = *p;
+          v.x ^= d.x;
+          v.y ^= d.y;
+        }
+        *p = v;
+      }
+    } else {  // rows 2h, 2h + 1: 4 bytes of 4 elements, transposed
+#pragma unroll
+      for (uint32_t jj = 0; jj < 2; ++jj) {
+        const uint32_t j = 2 * half + jj;
+        if (j >= a.m) break;
+        uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + off);
+        const uint32_t* o = &out[4 * jj];
+        uint4 v = make_uint4(row_word4(o, 0), row_word4(o, 1), row_word4(o, 2), row_word4(o, 3));
+        if (!a.overwrite) {
+          const uint4 d = *p;
+          v.x ^= d.x;
+          v.y ^= d.y;
+          v.z ^= d.z;
+          v.w ^= d.w;
+        }
+        *p = v;
+      }
+    }
+  }
+  return true;
+}
+
+template <int E>
+__device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, const uint32_t (&d_col)[2],
+                                              volatile int* abort) {
+  uint32_t out[8];  // output bytes 8h .. 8h + 7 of this thread's 4 columns
+#pragma unroll
+  for (int x = 0; x < 8; ++x) out[x] = 0;
+  StripeCursor cur;
+  bool ok = true;
+  for (uint64_t t = 0; t < ntiles && ok; t += 4) {
+    ok = epilogue<E, 0>(a, S, d_col, t, out, abort, cur);
+    if (ok) ok = epilogue<E, 1>(a, S, d_col, t + 1, out, abort, cur);
+    if (ok) ok = epilogue<E, 2>(a, S, d_col, t + 2, out, abort, cur);
+    if (ok) ok = epilogue<E, 3>(a, S, d_col, t + 3, out, abort, cur);
+  }
+  if (!ok) {
+    atomicExch(&g_gf2_err, 4);
     *abort = 1;
   }
 }
@@ -482,11 +513,12 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&S.full[s], 1);
-      mbar_init(&S.empty[s], kWorkerWarps);
+      mbar_init(&S.empty[s], kExpandWarps);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&S.afull[b], kWorkerWarps);
+      mbar_init(&S.afull[b], kExpandWarps);
       mbar_init(&S.dfull[b], 1);
+      mbar_init(&S.dempty[b], kWorkerWarps - kExpandWarps);
     }
     S.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -547,7 +579,9 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       uint64_t t = 0;
       for (; t < ntiles && !*abort; ++t) {
         const uint32_t b = static_cast<uint32_t>(t & 1u);
-        if (!mbar_wait(&S.afull[b], static_cast<uint32_t>((t >> 1) & 1u), abort)) {
+        // A of tile t written, and D of tile t - 2 read back
+        if (!mbar_wait(&S.afull[b], static_cast<uint32_t>((t >> 1) & 1u), abort) ||
+            (t >= 2 && !mbar_wait(&S.dempty[b], static_cast<uint32_t>(((t - 2) >> 1) & 1u), abort))) {
           atomicExch(&g_gf2_err, 2);
           *abort = 1;
           break;
@@ -561,9 +595,10 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       for (uint64_t u = t > 2 ? t - 2 : 0; u < t; ++u)
         mbar_wait(&S.dfull[u & 1u], static_cast<uint32_t>((u >> 1) & 1u), abort, false);
     }
+  } else if (warp < kExpandWarps) {
+    expander_loop<E>(a, S, stages, stage_bytes, nmine, a_col, abort);
   } else {
-    // ---- workers
-    worker_loop<E>(a, S, stages, stage_bytes, nmine, a_col, d_col, abort);
+    epilogue_loop<E>(a, S, ntiles, d_col, abort);
   }
   tc_fence_before();
   __syncthreads();
