@@ -173,6 +173,15 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
                : "memory");
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
@@ -244,80 +253,86 @@ __device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
 }
 
 struct Smem {
-  uint64_t full[kStages], empty[kStages], afull[2], dfull[2], dempty[2];
+  uint64_t full[kStages], empty[kStages], afull[4], aempty[4], dfull[3], dempty[3];
   uint32_t tmem_base;
   int abort;
 };
 
-// The 16 worker warps have two jobs. Expander warp e (0..7) and epilogue warp
-// e (8..15) own TMEM lanes 32 (e % 4) .. + 31, the element columns of a tile,
-// and half h = (e % 8) / 4 of their job: an expander writes input groups
-// 8h .. 8h + 7 of the A lanes (input bytes 32h .. 32h + 31), an epilogue warp
-// reads output bytes 8h .. 8h + 7 (D columns 64h .. 64h + 63). Expanders
-// refill A for tile t as soon as the product of tile t - 2 has finished
-// with it, while epilogue warps read that product back, so the chain between
-// two products is the longer of the two jobs, not their sum.
+// TMEM holds a ring of 4 A slots of 32 columns (4 input groups each, K = 128
+// per slot) and 3 D buffers of 128 columns. The issuer runs a tile's products
+// slot by slot (quarter j of the tile = input groups 4j .. 4j + 3) and
+// commits each slot back to the expanders as soon as its products are done,
+// so the expanders refill A up to a whole tile ahead of the products; D is
+// read back by the epilogue warps up to two tiles behind.
+constexpr uint32_t kSlots = 4;
+constexpr uint32_t kSlotCols = 32;
+constexpr uint32_t kDBufs = 3;
 
-// This half's groups of the A lane of tile Q (column 4i + Q of the block)
-// into TMEM buffer Q % 2. Group g = input bytes 4g..4g+3 of the column (input
-// byte u = t * E + p); TMEM column 8g + b holds bit b of those 4 bytes, each
-// as the value 2^b. sw holds this thread's words of input bytes 32h .. 32h +
-// 31 (global word 32h + x is sw[x]).
+// The 16 worker warps have two jobs. Expander warp e (0..7) and epilogue
+// warp e (8..15) own TMEM lanes 32 (e % 4) .. + 31, the element columns of a
+// tile, and half h = (e % 8) / 4 of their job: an expander writes input
+// groups 4j + 2h and 4j + 2h + 1 of every quarter j (16 TMEM columns), an
+// epilogue warp reads output bytes 8h .. 8h + 7 (D columns 64h .. 64h + 63).
+
+// Half h's two groups of quarter j of the A lane of tile Q (column 4i + Q of
+// the block) into the TMEM slot at a_col. Group g = input bytes 4g..4g+3 of
+// the column (input byte u = t * E + p); TMEM column 8g + b holds bit b of
+// those 4 bytes, each as the value 2^b. sw[8 c + x] is global word
+// 16 c + 8 h + x (c = quarter), i.e. this thread's words of the half's
+// groups.
 template <int E, int Q>
-__device__ __forceinline__ void expand(const Gf2Launch& a, const uint32_t (&sw)[32], uint32_t a_col, uint32_t half,
-                                       uint32_t lane_base) {
+__device__ __forceinline__ void expand_quarter(const Gf2Launch& a, const uint32_t (&sw)[32], uint32_t j,
+                                               uint32_t a_col, uint32_t half, uint32_t lane_base) {
+  const uint32_t g0 = 4u * j + 2u * half;
+  if (g0 >= a.ngroups) return;  // warp-uniform
   const uint32_t nwords = a.k * E;
+  uint32_t col[16];
 #pragma unroll
-  for (uint32_t c = 0; c < 2; ++c) {
-    const uint32_t g0 = 8u * half + 4u * c;
-    if (g0 >= a.ngroups) break;  // warp-uniform
-    uint32_t col[32];
+  for (uint32_t gg = 0; gg < 2; ++gg) {
+    const uint32_t gw = 4u * (g0 + gg);  // global word of the group's first input byte
+    uint32_t x[4];
 #pragma unroll
-    for (uint32_t gg = 0; gg < 4; ++gg) {
-      const uint32_t lw = 16u * c + 4u * gg;        // local word of the group's first input byte
-      const uint32_t gw = 32u * half + lw;          // global word
-      uint32_t wg;
-      if (E == 1) {  // sources 4g..4g+3, byte Q of each
-        constexpr uint32_t qs = Q | ((4u + Q) << 4);
-        const uint32_t s0 = gw < nwords ? sw[lw] : 0u;
-        const uint32_t s1 = gw + 1 < nwords ? sw[lw + 1] : 0u;
-        const uint32_t s2 = gw + 2 < nwords ? sw[lw + 2] : 0u;
-        const uint32_t s3 = gw + 3 < nwords ? sw[lw + 3] : 0u;
-        wg = prmt(prmt(s0, s1, qs), prmt(s2, s3, qs), 0x5410u);
-      } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
-        const uint32_t x0 = gw + Q / 2 < nwords ? sw[lw + Q / 2] : 0u;
-        const uint32_t x1 = gw + 2 + Q / 2 < nwords ? sw[lw + 2 + Q / 2] : 0u;
-        wg = prmt(x0, x1, (Q & 1) ? 0x7632u : 0x5410u);
-      } else {  // source g, element Q
-        wg = gw + Q < nwords ? sw[lw + Q] : 0u;
-      }
+    for (uint32_t y = 0; y < 4; ++y) {
+      // sw index of global word gw + y: quarter j, word 8h + 4gg + y within it
+      uint32_t v = 0;
 #pragma unroll
-      for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
+      for (uint32_t jj = 0; jj < 4; ++jj)
+        if (jj == j) v = sw[8 * jj + 4 * gg + y];
+      x[y] = gw + y < nwords ? v : 0u;
     }
-    const uint32_t taddr = lane_base | (a_col + 8u * g0);
-    if (a.ngroups - g0 >= 4) {
-      tmem_st32(taddr, col);
-    } else {
-#pragma unroll
-      for (uint32_t gg = 0; gg < 3; ++gg)
-        if (gg < a.ngroups - g0) tmem_st8(taddr + 8u * gg, &col[8 * gg]);
+    uint32_t wg;
+    if (E == 1) {  // sources 4g..4g+3, byte Q of each
+      constexpr uint32_t qs = Q | ((4u + Q) << 4);
+      wg = prmt(prmt(x[0], x[1], qs), prmt(x[2], x[3], qs), 0x5410u);
+    } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
+      wg = prmt(x[Q / 2], x[2 + Q / 2], (Q & 1) ? 0x7632u : 0x5410u);
+    } else {  // source g, element Q
+      wg = x[Q];
     }
+#pragma unroll
+    for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
   }
+  const uint32_t taddr = lane_base | (a_col + 8u * (2u * half));
+  if (a.ngroups - g0 >= 2)
+    tmem_st16(taddr, col);
+  else
+    tmem_st8(taddr, col);
   tmem_wait_st();
 }
 
 template <int E>
 __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
-                                              uint64_t nmine, const uint32_t (&a_col)[2], volatile int* abort) {
+                                              uint64_t nmine, uint32_t a_base, volatile int* abort) {
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t half = warp >> 2, i = (warp & 3u) * 32u + lane;
   const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  uint32_t sw[32];  // this thread's 4 columns of input bytes 32h .. 32h + 31
+  const uint32_t nq = (a.ngroups + 3u) / 4u;  // quarters per tile
+  uint32_t sw[32];  // sw[8 c + x] = global word 16 c + 8 h + x of this thread's 4 columns
 #pragma unroll
   for (int x = 0; x < 32; ++x) sw[x] = 0;
   const uint32_t nwords = a.k * E;
   bool ok = true;
-  uint64_t t = 0;  // tiles expanded so far
+  uint64_t qi = 0;  // slots filled so far
   for (uint64_t it = 0; it < nmine && ok; ++it) {
     const uint32_t s = static_cast<uint32_t>(it % kStages);
     if (!warp_wait(&S.full[s], static_cast<uint32_t>((it / kStages) & 1u), abort)) {
@@ -326,44 +341,45 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
     }
     const uint8_t* st = stages + s * stage_bytes;
 #pragma unroll
-    for (uint32_t w = 0; w < 32; w += E) {
-      const uint32_t gw = 32u * half + w;
-      if (gw >= nwords) break;
-      const uint8_t* p = st + (gw / E) * kCols * E + i * 4u * E;
-      if (E == 1) {
-        sw[w] = *reinterpret_cast<const uint32_t*>(p);
-      } else if (E == 2) {
-        const uint2 v = *reinterpret_cast<const uint2*>(p);
-        sw[w] = v.x;
-        sw[w + 1] = v.y;
-      } else {
-        const uint4 v = *reinterpret_cast<const uint4*>(p);
-        sw[w] = v.x;
-        sw[w + 1] = v.y;
-        sw[w + 2] = v.z;
-        sw[w + 3] = v.w;
+    for (uint32_t c = 0; c < 4; ++c)
+#pragma unroll
+      for (uint32_t x = 0; x < 8; x += E) {
+        const uint32_t gw = 16u * c + 8u * half + x;
+        if (gw >= nwords) break;
+        const uint8_t* p = st + (gw / E) * kCols * E + i * 4u * E;
+        if (E == 1) {
+          sw[8 * c + x] = *reinterpret_cast<const uint32_t*>(p);
+        } else if (E == 2) {
+          const uint2 v = *reinterpret_cast<const uint2*>(p);
+          sw[8 * c + x] = v.x;
+          sw[8 * c + x + 1] = v.y;
+        } else {
+          const uint4 v = *reinterpret_cast<const uint4*>(p);
+          sw[8 * c + x] = v.x;
+          sw[8 * c + x + 1] = v.y;
+          sw[8 * c + x + 2] = v.z;
+          sw[8 * c + x + 3] = v.w;
+        }
       }
-    }
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.empty[s]);  // the stage may be refilled
-    // tile Q of this block is tile t + Q: buffer Q % 2 is free once the
-    // product of tile t + Q - 2 has finished
-#define FGFC_TILE(Q)                                                                          \
-    if (ok && t + Q >= 2)                                                                     \
-      ok = warp_wait(&S.dfull[Q & 1], static_cast<uint32_t>(((t + Q - 2) >> 1) & 1u), abort); \
-    if (ok) {                                                                                 \
-      tc_fence_after();                                                                       \
-      expand<E, Q>(a, sw, a_col[Q & 1], half, lane_base);                                     \
-      tc_fence_before();                                                                      \
-      __syncwarp();                                                                           \
-      if (lane == 0) mbar_arrive(&S.afull[Q & 1]);                                            \
+#define FGFC_TILE(Q)                                                                                \
+    for (uint32_t j = 0; j < nq && ok; ++j, ++qi) {                                                 \
+      const uint32_t slot = static_cast<uint32_t>(qi % kSlots);                                     \
+      if (qi >= kSlots)                                                                             \
+        ok = warp_wait(&S.aempty[slot], static_cast<uint32_t>((qi / kSlots - 1) & 1u), abort);      \
+      if (!ok) break;                                                                               \
+      tc_fence_after();                                                                             \
+      expand_quarter<E, Q>(a, sw, j, a_base + kSlotCols * slot, half, lane_base);                   \
+      tc_fence_before();                                                                            \
+      __syncwarp();                                                                                 \
+      if (lane == 0) mbar_arrive(&S.afull[slot]);                                                   \
     }
     FGFC_TILE(0)
     FGFC_TILE(1)
     FGFC_TILE(2)
     FGFC_TILE(3)
 #undef FGFC_TILE
-    t += 4;
   }
   if (!ok) {
     atomicExch(&g_gf2_err, 3);
@@ -371,20 +387,21 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
   }
 }
 
-// Epilogue of tile tt (columns 4i + Q of its block, TMEM buffer Q % 2): read
+// Epilogue of tile tt (columns 4i + Q of its block, D buffer tt % 3): read
 // this half's accumulators and release the buffer, fold bit 7 of each into
 // output byte 8h + v of column Q (byte Q of out[v]); after the 4th tile
 // store 4 columns of this half's rows.
 template <int E, int Q>
-__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint32_t (&d_col)[2], uint64_t tt,
+__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, uint32_t d_base, uint64_t tt,
                                          uint32_t (&out)[8], volatile int* abort, StripeCursor& cur) {
-  constexpr uint32_t b = Q & 1;
   constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t half = (warp >> 2) & 1u, i = (warp & 3u) * 32u + lane;
   const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  if (!warp_wait(&S.dfull[b], static_cast<uint32_t>((tt >> 1) & 1u), abort)) return false;
+  const uint32_t d = static_cast<uint32_t>(tt % kDBufs);
+  if (!warp_wait(&S.dfull[d], static_cast<uint32_t>((tt / kDBufs) & 1u), abort)) return false;
   tc_fence_after();
+  const uint32_t d_col = d_base + 128u * d;
   const uint32_t c0 = 64u * half;
   const uint32_t nout = a.m * E;
   // two 32-column loads, one at a time (registers), then the buffer is released
@@ -394,9 +411,9 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
     if (cc < a.npad) {  // warp-uniform
       uint32_t r[32];
       if (a.npad - cc >= 32) {
-        tmem_ld32(lane_base | (d_col[b] + cc), r);
+        tmem_ld32(lane_base | (d_col + cc), r);
       } else {
-        tmem_ld16(lane_base | (d_col[b] + cc), r);
+        tmem_ld16(lane_base | (d_col + cc), r);
 #pragma unroll
         for (int x = 16; x < 32; ++x) r[x] = 0;
       }
@@ -408,7 +425,7 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
   }
   tc_fence_before();
   __syncwarp();
-  if (lane == 0) mbar_arrive(&S.dempty[b]);  // the next product may overwrite D
+  if (lane == 0) mbar_arrive(&S.dempty[d]);  // a later product may overwrite D
   if (c0 >= a.npad) return true;
   if (Q == 3) {
     const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
@@ -429,9 +446,9 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
         uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + off);
         uint2 v = make_uint2(prmt(out[2 * jj], out[2 * jj + 1], 0x5140u), prmt(out[2 * jj], out[2 * jj + 1], 0x7362u));
         if (!a.overwrite) {
-          const uint2 d = *p;
-          v.x ^= d.x;
-          v.y ^= d.y;
+          const uint2 dd = *p;
+          v.x ^= dd.x;
+          v.y ^= dd.y;
         }
         *p = v;
       }
@@ -444,11 +461,11 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
         const uint32_t* o = &out[4 * jj];
         uint4 v = make_uint4(row_word4(o, 0), row_word4(o, 1), row_word4(o, 2), row_word4(o, 3));
         if (!a.overwrite) {
-          const uint4 d = *p;
-          v.x ^= d.x;
-          v.y ^= d.y;
-          v.z ^= d.z;
-          v.w ^= d.w;
+          const uint4 dd = *p;
+          v.x ^= dd.x;
+          v.y ^= dd.y;
+          v.z ^= dd.z;
+          v.w ^= dd.w;
         }
         *p = v;
       }
@@ -458,7 +475,7 @@ __device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, const uint
 }
 
 template <int E>
-__device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, const uint32_t (&d_col)[2],
+__device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, uint32_t d_base,
                                               volatile int* abort) {
   uint32_t out[8];  // output bytes 8h .. 8h + 7 of this thread's 4 columns
 #pragma unroll
@@ -466,10 +483,10 @@ __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint6
   StripeCursor cur;
   bool ok = true;
   for (uint64_t t = 0; t < ntiles && ok; t += 4) {
-    ok = epilogue<E, 0>(a, S, d_col, t, out, abort, cur);
-    if (ok) ok = epilogue<E, 1>(a, S, d_col, t + 1, out, abort, cur);
-    if (ok) ok = epilogue<E, 2>(a, S, d_col, t + 2, out, abort, cur);
-    if (ok) ok = epilogue<E, 3>(a, S, d_col, t + 3, out, abort, cur);
+    ok = epilogue<E, 0>(a, S, d_base, t, out, abort, cur);
+    if (ok) ok = epilogue<E, 1>(a, S, d_base, t + 1, out, abort, cur);
+    if (ok) ok = epilogue<E, 2>(a, S, d_base, t + 2, out, abort, cur);
+    if (ok) ok = epilogue<E, 3>(a, S, d_base, t + 3, out, abort, cur);
   }
   if (!ok) {
     atomicExch(&g_gf2_err, 4);
@@ -515,10 +532,13 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], kExpandWarps);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&S.afull[b], kExpandWarps);
-      mbar_init(&S.dfull[b], 1);
-      mbar_init(&S.dempty[b], kWorkerWarps - kExpandWarps);
+    for (uint32_t s = 0; s < kSlots; ++s) {
+      mbar_init(&S.afull[s], kExpandWarps);
+      mbar_init(&S.aempty[s], 1);
+    }
+    for (uint32_t d = 0; d < kDBufs; ++d) {
+      mbar_init(&S.dfull[d], 1);
+      mbar_init(&S.dempty[d], kWorkerWarps - kExpandWarps);
     }
     S.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -535,8 +555,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = S.tmem_base;
-  const uint32_t a_col[2] = {tbase, tbase + 128u};
-  const uint32_t d_col[2] = {tbase + 256u, tbase + 384u};
+  const uint32_t a_base = tbase;                        // 4 slots x 32 columns
+  const uint32_t d_base = tbase + kSlots * kSlotCols;   // 3 buffers x 128 columns
 
   // blocks of this CTA: blockIdx.x, + gridDim.x, ...
   const uint64_t nmine = a.nblk > blockIdx.x ? (a.nblk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
@@ -571,34 +591,48 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       for (uint64_t i = issued > kStages ? issued - kStages : 0; i < issued; ++i)
         mbar_wait(&S.full[i % kStages], static_cast<uint32_t>((i / kStages) & 1u), abort, false);
   } else if (warp == kIssuerWarp) {
-    // ---- issuer: one thread issues every product of a tile
+    // ---- issuer: one thread issues every product, slot by slot
     if (lane == 0) {
       const uint32_t idesc = (2u << 4) | ((a.npad >> 3) << 17) | ((128u >> 4) << 24);  // s32 += u8 * u8, M = 128
       const uint32_t bsm = smem_u32(bimg);
       const uint32_t lbo = a.npad * 16u, sbo = 128u;
-      uint64_t t = 0;
-      for (; t < ntiles && !*abort; ++t) {
-        const uint32_t b = static_cast<uint32_t>(t & 1u);
-        // A of tile t written, and D of tile t - 2 read back
-        if (!mbar_wait(&S.afull[b], static_cast<uint32_t>((t >> 1) & 1u), abort) ||
-            (t >= 2 && !mbar_wait(&S.dempty[b], static_cast<uint32_t>(((t - 2) >> 1) & 1u), abort))) {
-          atomicExch(&g_gf2_err, 2);
-          *abort = 1;
+      const uint32_t nq = (a.ngroups + 3u) / 4u;
+      uint64_t t = 0, qi = 0;
+      bool ok = true;
+      for (; t < ntiles && ok; ++t) {
+        const uint32_t d = static_cast<uint32_t>(t % kDBufs);
+        if (t >= kDBufs && !mbar_wait(&S.dempty[d], static_cast<uint32_t>((t / kDBufs - 1) & 1u), abort)) {
+          ok = false;
           break;
         }
-        tc_fence_after();
-        for (uint32_t g = 0; g < a.ngroups; ++g)
-          mma_i8(d_col[b], a_col[b] + 8u * g, smem_desc(bsm + g * 2u * a.npad * 16u, lbo, sbo), idesc, g > 0);
-        mma_commit(&S.dfull[b]);
+        for (uint32_t j = 0; j < nq; ++j, ++qi) {
+          const uint32_t slot = static_cast<uint32_t>(qi % kSlots);
+          if (!mbar_wait(&S.afull[slot], static_cast<uint32_t>((qi / kSlots) & 1u), abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t gend = min(a.ngroups, 4u * j + 4u);
+          for (uint32_t g = 4u * j; g < gend; ++g)
+            mma_i8(d_base + 128u * d, a_base + kSlotCols * slot + 8u * (g - 4u * j),
+                   smem_desc(bsm + g * 2u * a.npad * 16u, lbo, sbo), idesc, g > 0);
+          mma_commit(&S.aempty[slot]);  // this slot may be refilled once its products are done
+        }
+        if (!ok) break;
+        mma_commit(&S.dfull[d]);
+      }
+      if (!ok) {
+        atomicExch(&g_gf2_err, 2);
+        *abort = 1;
       }
       // the last products must finish before TMEM is freed
-      for (uint64_t u = t > 2 ? t - 2 : 0; u < t; ++u)
-        mbar_wait(&S.dfull[u & 1u], static_cast<uint32_t>((u >> 1) & 1u), abort, false);
+      for (uint64_t u = t > kDBufs ? t - kDBufs : 0; u < t; ++u)
+        mbar_wait(&S.dfull[u % kDBufs], static_cast<uint32_t>((u / kDBufs) & 1u), abort, false);
     }
   } else if (warp < kExpandWarps) {
-    expander_loop<E>(a, S, stages, stage_bytes, nmine, a_col, abort);
+    expander_loop<E>(a, S, stages, stage_bytes, nmine, a_base, abort);
   } else {
-    epilogue_loop<E>(a, S, ntiles, d_col, abort);
+    epilogue_loop<E>(a, S, ntiles, d_base, abort);
   }
   tc_fence_before();
   __syncthreads();
