@@ -252,21 +252,23 @@ __device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
   return (p03 >> 4) * 0x00204081u + p47 * 0x00204081u;  // output byte in bits 24..31
 }
 
+// TMEM holds a ring of 8 A slots of 32 columns (4 input groups each, K = 128
+// per slot) and 2 D buffers of 128 columns. The issuer runs a tile's products
+// slot by slot (quarter j of the tile = input groups 4j .. 4j + 3) and
+// commits each slot back to the expanders as soon as its products are done,
+// so the expanders refill A up to two tiles ahead of the products; D is read
+// back by the epilogue warps one tile behind.
+constexpr uint32_t kSlots = 8;
+constexpr uint32_t kSlotCols = 32;
+constexpr uint32_t kDBufs = 2;
+static_assert(kSlots * kSlotCols + kDBufs * 128u <= kTmemCols, "TMEM budget");
+
 struct Smem {
-  uint64_t full[kStages], empty[kStages], afull[4], aempty[4], dfull[3], dempty[3];
+  uint64_t full[kStages], empty[kStages], afull[kSlots], aempty[kSlots], dfull[kDBufs], dempty[kDBufs];
   uint32_t tmem_base;
   int abort;
 };
 
-// TMEM holds a ring of 4 A slots of 32 columns (4 input groups each, K = 128
-// per slot) and 3 D buffers of 128 columns. The issuer runs a tile's products
-// slot by slot (quarter j of the tile = input groups 4j .. 4j + 3) and
-// commits each slot back to the expanders as soon as its products are done,
-// so the expanders refill A up to a whole tile ahead of the products; D is
-// read back by the epilogue warps up to two tiles behind.
-constexpr uint32_t kSlots = 4;
-constexpr uint32_t kSlotCols = 32;
-constexpr uint32_t kDBufs = 3;
 
 // The 16 worker warps have two jobs. Expander warp e (0..7) and epilogue
 // warp e (8..15) own TMEM lanes 32 (e % 4) .. + 31, the element columns of a
@@ -555,8 +557,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = S.tmem_base;
-  const uint32_t a_base = tbase;                        // 4 slots x 32 columns
-  const uint32_t d_base = tbase + kSlots * kSlotCols;   // 3 buffers x 128 columns
+  const uint32_t a_base = tbase;                        // kSlots slots x 32 columns
+  const uint32_t d_base = tbase + kSlots * kSlotCols;   // kDBufs buffers x 128 columns
 
   // blocks of this CTA: blockIdx.x, + gridDim.x, ...
   const uint64_t nmine = a.nblk > blockIdx.x ? (a.nblk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
