@@ -5,35 +5,40 @@
 // the 8E output bits of c * x are XORs of the 8E input bits of x. So for one
 // element column (one element position of every source and row) the whole
 // op rows[j] (^)= XOR_t c[t][j] * src_t is one GF(2) matrix-vector product:
-// out (8E * m bits) = B (8E*m x 8E*k) . in (8E*k bits). It is evaluated as an
-// integer matrix product whose low bit is the parity:
+// out (8E * m bits) = A (8E*m x 8E*k) . in (8E*k bits). It is evaluated as an
+// integer matrix product whose bit 7 is the parity:
 //
-//   D[col][n] = sum_kappa A[col][kappa] * B[kappa][n]     (tcgen05.mma kind::i8)
+//   D[n][col] = sum_kappa A[n][kappa] * B[kappa][col]     (tcgen05.mma kind::i8)
 //
-// with A the input bits of 128 element columns (M = 128, one TMEM lane per
-// column) and B the plan's bit matrix (N = output bits, K = input bits). The
-// input bit b of a byte enters A as the value 2^b (the byte masked with
-// 0x01010101 << b, one LOP3 per 4 values) and B holds 2^(7-b) where the bit
-// matrix has a 1, so every product is 0 or 128 and D = 128 * (number of 1
+// with A the plan's bit matrix (M = 128 output bits, one TMEM lane each, rows
+// past the 8E*m real ones zero; K = input bits) and B the input bits of 256
+// element columns (N = 256). Putting the columns on N makes every product the
+// largest the instruction takes (M = 128, N = 256, K = 32); its cost on this
+// part hardly depends on N, so fewer, wider products are what the contraction
+// needs. The input bit b of a byte enters B as the value 2^b (the byte masked
+// with 0x01010101 << b, one LOP3 per 4 values) and A holds 2^(7-b) where the
+// bit matrix has a 1, so every product is 0 or 128 and D = 128 * (number of 1
 // products): its bit 7 is the GF(2) sum, bits 0..6 are zero. Sums stay below
 // 2^23 (at most 512 products of 2^14), so the int32 accumulator is exact.
 //
-// Layout and flow of one CTA (one per SM, persistent over 512-column blocks):
-//   * the producer warp stages the k source rows of a block (512 columns,
-//     512 * E bytes per source) into a 4-deep shared-memory ring with
-//     cp.async.bulk (single GPU, no multicast), completion on an mbarrier;
-//   * warps 0..7 (expanders; thread i of a lane quarter owns TMEM lane i):
-//     read the 4 consecutive columns 4i..4i+3 of their half of the sources
-//     into registers, then for each of the block's 4 tiles (tile q = columns
-//     4i + q) build their half of the A lane and write it with tcgen05.st;
-//   * warps 8..15 (epilogue): when a tile's product is done, read their half
-//     of D back (tcgen05.ld), release the buffer, gather bit 7 of every
-//     accumulator into output bytes with PRMT and two multiply-adds, and
-//     after the 4th tile store 4 consecutive columns of their rows;
-//   * warp 16 (producer): see above, every lane issuing copies;
-//   * warp 17 (issuer): allocates TMEM (A and D double-buffered, 512 columns),
-//     issues K/32 tcgen05.mma per tile from one thread and commits each tile
-//     to an mbarrier.
+// Layout and flow of one CTA (one per SM, persistent over 512-column blocks,
+// two 256-column tiles each):
+//   * the producer warp stages the k source rows of a block (512 * E bytes
+//     per source) into a 2..4-deep shared-memory ring with cp.async.bulk
+//     (single GPU, no multicast), completion on an mbarrier;
+//   * warps 0..7 (expanders; thread i owns column i of a tile): gather the
+//     column's input bytes from the stage and write its expanded input bits
+//     into a ring of B slots in shared memory (4 input groups, K = 128, per
+//     slot), each slot handed to the issuer through an mbarrier;
+//   * warp 13 (issuer): allocates TMEM (two D buffers of 256 columns),
+//     issues the K/32 products of a tile from one lane, A and B
+//     both from shared memory, commits each slot back to the expanders once
+//     its products are done and the tile to the epilogue;
+//   * warps 8..11 (epilogue, one per TMEM lane quarter = 4 output bytes):
+//     read D back 32 columns at a time (tcgen05.ld), turn bit 7 of the 32
+//     lanes into the column's 4 output bytes with one ballot, release D and
+//     store 8 consecutive columns per lane;
+//   * warp 12 (producer): see above, every lane issuing copies.
 // Every mbarrier wait is bounded: a wait that runs out sets the error word,
 // stops the CTA's loops, waits (bounded) for its own copies and products in
 // flight and frees TMEM before returning.
@@ -52,15 +57,14 @@ namespace fgfc {
 
 namespace {
 
-constexpr int kExpandWarps = 8;                        // warps 0 .. 7: write A lanes
-constexpr int kWorkerWarps = 16;                       // + warps 8 .. 15: read D back
-constexpr int kProducerWarp = kWorkerWarps;            // bulk copies of source blocks
-constexpr int kIssuerWarp = kWorkerWarps + 1;          // TMEM allocation and the products
-constexpr int kMmaThreads = (kWorkerWarps + 2) * 32;   // 576
-constexpr int kStages = 4;
-constexpr uint32_t kCols = 512;        // element columns per block (4 tiles of 128)
+constexpr int kExpandWarps = 8;                        // warps 0 .. 7: expand inputs into B slots
+constexpr int kEpilogueWarps = 4;                      // warps 8 .. 11: read D back, one per lane quarter
+constexpr int kProducerWarp = kExpandWarps + kEpilogueWarps;  // bulk copies of source blocks
+constexpr int kIssuerWarp = kProducerWarp + 1;         // TMEM allocation and the products
+constexpr int kMmaThreads = (kIssuerWarp + 1) * 32;    // 448
+constexpr uint32_t kCols = 512;        // element columns per block (2 tiles of 256)
 constexpr uint32_t kMaxInBits = 512;   // K
-constexpr uint32_t kMaxOutBits = 128;  // N
+constexpr uint32_t kMaxOutBits = 128;  // M
 constexpr uint32_t kTmemCols = 512;
 constexpr int kMaxLaunchSmem = 227 * 1024;  // the opt-in every launch fits under
 constexpr uint64_t kWaitNs = 2000000000ull;   // 2 s: a wait this long means the pipeline is stuck
@@ -76,7 +80,7 @@ struct Gf2Launch {
   uint64_t nblk;                // 512-column blocks
   uint32_t k, m, E;
   uint32_t ngroups;             // K / 32: groups of 4 input bytes
-  uint32_t npad;                // N: output bits padded to a multiple of 16
+  uint32_t nstages, nslots;     // source stages and B slots in shared memory
   uint32_t overwrite;
   // Several stripes sharing this plan (nstripes > 0): stripe s owns blocks
   // [prefix[s], prefix[s + 1]) and its k source and m row pointers are
@@ -156,33 +160,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
-      "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
-      "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
-               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
-          taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* v) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
       "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -194,16 +172,6 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* v) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
@@ -214,13 +182,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
+__device__ __forceinline__ void mma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -243,145 +211,114 @@ struct StripeCursor {
   }
 };
 
-// Output byte from 8 accumulators (bit o of the byte = bit 7 of r[o]).
-__device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
-  const uint32_t p03 = prmt(prmt(r[0], r[1], 0x0040u), prmt(r[2], r[3], 0x0040u), 0x5410u);
-  const uint32_t p47 = prmt(prmt(r[4], r[5], 0x0040u), prmt(r[6], r[7], 0x0040u), 0x5410u);
-  // bit 7 of byte i of p03 -> bit 24 + i; of p47 -> bit 28 + i (no carries:
-  // every shifted copy lands on a distinct bit)
-  return (p03 >> 4) * 0x00204081u + p47 * 0x00204081u;  // output byte in bits 24..31
-}
-
-// TMEM holds a ring of 8 A slots of 32 columns (4 input groups each, K = 128
-// per slot) and 2 D buffers of 128 columns. The issuer runs a tile's products
-// slot by slot (quarter j of the tile = input groups 4j .. 4j + 3) and
-// commits each slot back to the expanders as soon as its products are done,
-// so the expanders refill A up to two tiles ahead of the products; D is read
-// back by the epilogue warps one tile behind.
-constexpr uint32_t kSlots = 8;
-constexpr uint32_t kSlotCols = 32;
-constexpr uint32_t kDBufs = 2;
-static_assert(kSlots * kSlotCols + kDBufs * 128u <= kTmemCols, "TMEM budget");
+// Shared memory of a CTA: [A image: the bit matrix, 4 KiB per input group]
+// [B slots: kSlotGroups groups of expanded inputs each, 8 KiB per group]
+// [source stages: one 512-column block of every source each] [Smem].
+// TMEM holds two D buffers of 256 columns (one per tile in flight).
+constexpr uint32_t kTileCols = 256;                  // N: element columns per product
+constexpr uint32_t kSlotGroups = 4;                  // input groups (K = 128) per B slot
+constexpr uint32_t kGroupBytes = kTileCols * 32u;    // one group of a tile: 256 columns x 32 K-bytes
+constexpr uint32_t kSlotBytes = kSlotGroups * kGroupBytes;
+constexpr uint32_t kABytesPerGroup = 128u * 32u;     // M = 128 output bits x 32 K-bytes
+constexpr int kMaxStages = 4;
+constexpr int kMaxSlots = 6;
+constexpr uint32_t kDBufs = 2;  // the issuer and epilogue index D by t & 1
+static_assert(kDBufs * kTileCols <= kTmemCols, "TMEM budget");
 
 struct Smem {
-  uint64_t full[kStages], empty[kStages], afull[kSlots], aempty[kSlots], dfull[kDBufs], dempty[kDBufs];
+  uint64_t full[kMaxStages], empty[kMaxStages], bfull[kMaxSlots], bempty[kMaxSlots], dfull[kDBufs], dempty[kDBufs];
   uint32_t tmem_base;
   int abort;
 };
 
-
-// The 16 worker warps have two jobs. Expander warp e (0..7) and epilogue
-// warp e (8..15) own TMEM lanes 32 (e % 4) .. + 31, the element columns of a
-// tile, and half h = (e % 8) / 4 of their job: an expander writes input
-// groups 4j + 2h and 4j + 2h + 1 of every quarter j (16 TMEM columns), an
-// epilogue warp reads output bytes 8h .. 8h + 7 (D columns 64h .. 64h + 63).
-
-// Half h's two groups of quarter j of the A lane of tile Q (column 4i + Q of
-// the block) into the TMEM slot at a_col. Group g = input bytes 4g..4g+3 of
-// the column (input byte u = t * E + p); TMEM column 8g + b holds bit b of
-// those 4 bytes, each as the value 2^b. sw[8 c + x] is global word
-// 16 c + 8 h + x (c = quarter), i.e. this thread's words of the half's
-// groups.
-template <int E, int Q>
-__device__ __forceinline__ void expand_quarter(const Gf2Launch& a, const uint32_t (&sw)[32], uint32_t j,
-                                               uint32_t a_col, uint32_t half, uint32_t lane_base) {
-  const uint32_t g0 = 4u * j + 2u * half;
-  if (g0 >= a.ngroups) return;  // warp-uniform
-  const uint32_t nwords = a.k * E;
-  uint32_t col[16];
-#pragma unroll
-  for (uint32_t gg = 0; gg < 2; ++gg) {
-    const uint32_t gw = 4u * (g0 + gg);  // global word of the group's first input byte
-    uint32_t x[4];
-#pragma unroll
-    for (uint32_t y = 0; y < 4; ++y) {
-      // sw index of global word gw + y: quarter j, word 8h + 4gg + y within it
-      uint32_t v = 0;
-#pragma unroll
-      for (uint32_t jj = 0; jj < 4; ++jj)
-        if (jj == j) v = sw[8 * jj + 4 * gg + y];
-      x[y] = gw + y < nwords ? v : 0u;
+// Position in a ring of n barrier-guarded buffers: the buffer index and the
+// phase parity of its current use; `reused` once a full turn has been made
+// (from then on a buffer must be released before it is filled again). Kept
+// incrementally: the loops that walk the rings do no division.
+struct Ring {
+  uint32_t n, i = 0, ph = 0;
+  bool reused = false;
+  __device__ __forceinline__ explicit Ring(uint32_t count) : n(count) {}
+  __device__ __forceinline__ void next() {
+    if (++i == n) {
+      i = 0;
+      ph ^= 1u;
+      reused = true;
     }
-    uint32_t wg;
-    if (E == 1) {  // sources 4g..4g+3, byte Q of each
-      constexpr uint32_t qs = Q | ((4u + Q) << 4);
-      wg = prmt(prmt(x[0], x[1], qs), prmt(x[2], x[3], qs), 0x5410u);
-    } else if (E == 2) {  // sources 2g, 2g+1: element Q is word Q / 2, bytes 2 (Q % 2) .. + 1
-      wg = prmt(x[Q / 2], x[2 + Q / 2], (Q & 1) ? 0x7632u : 0x5410u);
-    } else {  // source g, element Q
-      wg = x[Q];
-    }
-#pragma unroll
-    for (uint32_t bb = 0; bb < 8; ++bb) col[gg * 8 + bb] = wg & (0x01010101u << bb);
   }
-  const uint32_t taddr = lane_base | (a_col + 8u * (2u * half));
-  if (a.ngroups - g0 >= 2)
-    tmem_st16(taddr, col);
-  else
-    tmem_st8(taddr, col);
-  tmem_wait_st();
+};
+
+__device__ __forceinline__ void sts128(uint32_t addr, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
 }
 
+// Input bytes 4g .. 4g + 3 of element column `col` of the staged block
+// (input byte u = t * E + p: byte p of source t's element), byte r of the
+// result = input byte 4g + r; bytes past the k * E input bytes are zero.
+template <int E>
+__device__ __forceinline__ uint32_t gather_group(const uint8_t* st, uint32_t g, uint32_t col, uint32_t k) {
+  if (E == 1) {
+    uint32_t v = 0;
+#pragma unroll
+    for (uint32_t r = 0; r < 4; ++r) {
+      const uint32_t t = 4u * g + r;
+      if (t < k) v |= static_cast<uint32_t>(st[t * kCols + col]) << (8 * r);
+    }
+    return v;
+  } else if (E == 2) {
+    const uint32_t t = 2u * g;
+    const uint32_t lo = reinterpret_cast<const uint16_t*>(st + t * kCols * 2u)[col];
+    const uint32_t hi = t + 1 < k ? reinterpret_cast<const uint16_t*>(st + (t + 1) * kCols * 2u)[col] : 0u;
+    return lo | (hi << 16);
+  } else {
+    return reinterpret_cast<const uint32_t*>(st + g * kCols * 4u)[col];
+  }
+}
+
+// Expander warps 0..7: thread i owns element column i of every tile. For each
+// B slot of a tile it writes the slot's groups of its column: group g, bit b
+// of input byte 4g + r becomes K-byte 4b + r of the group with the value 2^b
+// (the 4 input bytes masked with 0x01010101 << b), K-bytes 0..15 and 16..31
+// in the two 16-byte halves of the column's row (LBO apart).
 template <int E>
 __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const uint8_t* stages, uint32_t stage_bytes,
-                                              uint64_t nmine, uint32_t a_base, volatile int* abort) {
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t half = warp >> 2, i = (warp & 3u) * 32u + lane;
-  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  const uint32_t nq = (a.ngroups + 3u) / 4u;  // quarters per tile
-  uint32_t sw[32];  // sw[8 c + x] = global word 16 c + 8 h + x of this thread's 4 columns
-#pragma unroll
-  for (int x = 0; x < 32; ++x) sw[x] = 0;
-  const uint32_t nwords = a.k * E;
+                                              uint32_t nstages, uint32_t slots, uint32_t nslots, uint64_t nmine,
+                                              volatile int* abort) {
+  const uint32_t i = threadIdx.x, lane = i & 31u;
+  const uint32_t nq = (a.ngroups + kSlotGroups - 1) / kSlotGroups;  // slots per tile
   bool ok = true;
-  uint64_t qi = 0;  // slots filled so far
-  for (uint64_t it = 0; it < nmine && ok; ++it) {
-    const uint32_t s = static_cast<uint32_t>(it % kStages);
-    if (!warp_wait(&S.full[s], static_cast<uint32_t>((it / kStages) & 1u), abort)) {
+  Ring st(nstages), sl(nslots);
+  for (uint64_t it = 0; it < nmine && ok; ++it, st.next()) {
+    if (!warp_wait(&S.full[st.i], st.ph, abort)) {
       ok = false;
       break;
     }
-    const uint8_t* st = stages + s * stage_bytes;
-#pragma unroll
-    for (uint32_t c = 0; c < 4; ++c)
-#pragma unroll
-      for (uint32_t x = 0; x < 8; x += E) {
-        const uint32_t gw = 16u * c + 8u * half + x;
-        if (gw >= nwords) break;
-        const uint8_t* p = st + (gw / E) * kCols * E + i * 4u * E;
-        if (E == 1) {
-          sw[8 * c + x] = *reinterpret_cast<const uint32_t*>(p);
-        } else if (E == 2) {
-          const uint2 v = *reinterpret_cast<const uint2*>(p);
-          sw[8 * c + x] = v.x;
-          sw[8 * c + x + 1] = v.y;
-        } else {
-          const uint4 v = *reinterpret_cast<const uint4*>(p);
-          sw[8 * c + x] = v.x;
-          sw[8 * c + x + 1] = v.y;
-          sw[8 * c + x + 2] = v.z;
-          sw[8 * c + x + 3] = v.w;
+    const uint8_t* stp = stages + st.i * stage_bytes;
+    for (uint32_t T = 0; T < kCols / kTileCols && ok; ++T) {
+      const uint32_t col = T * kTileCols + i;
+      for (uint32_t j = 0; j < nq; ++j, sl.next()) {
+        if (sl.reused && !warp_wait(&S.bempty[sl.i], sl.ph ^ 1u, abort)) {
+          ok = false;
+          break;
         }
+        const uint32_t sbase = slots + sl.i * kSlotBytes + i * 16u;
+#pragma unroll
+        for (uint32_t gg = 0; gg < kSlotGroups; ++gg) {
+          const uint32_t g = kSlotGroups * j + gg;
+          if (g >= a.ngroups) break;  // uniform
+          const uint32_t w = gather_group<E>(stp, g, col, a.k);
+          const uint32_t base = sbase + gg * kGroupBytes;
+          sts128(base, w & 0x01010101u, w & 0x02020202u, w & 0x04040404u, w & 0x08080808u);
+          sts128(base + kGroupBytes / 2, w & 0x10101010u, w & 0x20202020u, w & 0x40404040u, w & 0x80808080u);
+        }
+        // generic-proxy writes become visible to the tensor cores' reads
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&S.bfull[sl.i]);
       }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&S.empty[s]);  // the stage may be refilled
-#define FGFC_TILE(Q)                                                                                \
-    for (uint32_t j = 0; j < nq && ok; ++j, ++qi) {                                                 \
-      const uint32_t slot = static_cast<uint32_t>(qi % kSlots);                                     \
-      if (qi >= kSlots)                                                                             \
-        ok = warp_wait(&S.aempty[slot], static_cast<uint32_t>((qi / kSlots - 1) & 1u), abort);      \
-      if (!ok) break;                                                                               \
-      tc_fence_after();                                                                             \
-      expand_quarter<E, Q>(a, sw, j, a_base + kSlotCols * slot, half, lane_base);                   \
-      tc_fence_before();                                                                            \
-      __syncwarp();                                                                                 \
-      if (lane == 0) mbar_arrive(&S.afull[slot]);                                                   \
     }
-    FGFC_TILE(0)
-    FGFC_TILE(1)
-    FGFC_TILE(2)
-    FGFC_TILE(3)
-#undef FGFC_TILE
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.empty[st.i]);  // both tiles read: the stage may be refilled
   }
   if (!ok) {
     atomicExch(&g_gf2_err, 3);
@@ -389,106 +326,99 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
   }
 }
 
-// Epilogue of tile tt (columns 4i + Q of its block, D buffer tt % 3): read
-// this half's accumulators and release the buffer, fold bit 7 of each into
-// output byte 8h + v of column Q (byte Q of out[v]); after the 4th tile
-// store 4 columns of this half's rows.
-template <int E, int Q>
-__device__ __forceinline__ bool epilogue(const Gf2Launch& a, Smem& S, uint32_t d_base, uint64_t tt,
-                                         uint32_t (&out)[8], volatile int* abort, StripeCursor& cur) {
-  constexpr uint32_t qsel = (0x3210u & ~(0xFu << (4 * Q))) | (7u << (4 * Q));  // byte Q <- byte 3 of the pack
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t half = (warp >> 2) & 1u, i = (warp & 3u) * 32u + lane;
-  const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
-  const uint32_t d = static_cast<uint32_t>(tt % kDBufs);
-  if (!warp_wait(&S.dfull[d], static_cast<uint32_t>((tt / kDBufs) & 1u), abort)) return false;
-  tc_fence_after();
-  const uint32_t d_col = d_base + 128u * d;
-  const uint32_t c0 = 64u * half;
-  const uint32_t nout = a.m * E;
-  // two 32-column loads, one at a time (registers), then the buffer is released
+// Output words of 8 consecutive columns (w[x] = output bytes 4q .. 4q + 3 of
+// column col0 + x, byte i = output byte 4q + i) into the rows they belong to.
+template <int E>
+__device__ __forceinline__ void store_columns(const Gf2Launch& a, StripeCursor& cur, uint64_t blk, uint32_t colb,
+                                              uint32_t q, const uint32_t (&w)[8]) {
+  if (E == 4) {  // row q: 8 elements
+    if (q >= a.m) return;
+    uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + q) + colb * 4u);
+    uint4 v0 = make_uint4(w[0], w[1], w[2], w[3]), v1 = make_uint4(w[4], w[5], w[6], w[7]);
+    if (!a.overwrite) {
+      const uint4 d0 = p[0], d1 = p[1];
+      v0.x ^= d0.x; v0.y ^= d0.y; v0.z ^= d0.z; v0.w ^= d0.w;
+      v1.x ^= d1.x; v1.y ^= d1.y; v1.z ^= d1.z; v1.w ^= d1.w;
+    }
+    p[0] = v0;
+    p[1] = v1;
+  } else if (E == 2) {  // rows 2q (low halves) and 2q + 1 (high halves)
 #pragma unroll
-  for (uint32_t c = 0; c < 2; ++c) {
-    const uint32_t cc = c0 + 32u * c;
-    if (cc < a.npad) {  // warp-uniform
-      uint32_t r[32];
-      if (a.npad - cc >= 32) {
-        tmem_ld32(lane_base | (d_col + cc), r);
-      } else {
-        tmem_ld16(lane_base | (d_col + cc), r);
-#pragma unroll
-        for (int x = 16; x < 32; ++x) r[x] = 0;
+    for (uint32_t h = 0; h < 2; ++h) {
+      const uint32_t j = 2u * q + h;
+      if (j >= a.m) break;
+      const uint32_t sel = h ? 0x7632u : 0x5410u;
+      uint4 v = make_uint4(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel), prmt(w[4], w[5], sel), prmt(w[6], w[7], sel));
+      uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + colb * 2u);
+      if (!a.overwrite) {
+        const uint4 d = *p;
+        v.x ^= d.x; v.y ^= d.y; v.z ^= d.z; v.w ^= d.w;
       }
-      tmem_wait_ld();
+      *p = v;
+    }
+  } else {  // rows 4q + r: byte r of every word
 #pragma unroll
-      for (uint32_t v = 0; v < 4; ++v)
-        if (8 * half + 4 * c + v < nout) out[4 * c + v] = prmt(out[4 * c + v], pack_byte(&r[8 * v]), qsel);
+    for (uint32_t r = 0; r < 4; ++r) {
+      const uint32_t j = 4u * q + r;
+      if (j >= a.m) break;
+      const uint32_t sel = r | ((4u + r) << 4);
+      uint2 v = make_uint2(prmt(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel), 0x5410u),
+                           prmt(prmt(w[4], w[5], sel), prmt(w[6], w[7], sel), 0x5410u));
+      uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + colb);
+      if (!a.overwrite) {
+        const uint2 d = *p;
+        v.x ^= d.x;
+        v.y ^= d.y;
+      }
+      *p = v;
     }
   }
-  tc_fence_before();
-  __syncwarp();
-  if (lane == 0) mbar_arrive(&S.dempty[d]);  // a later product may overwrite D
-  if (c0 >= a.npad) return true;
-  if (Q == 3) {
-    const uint64_t blk = blockIdx.x + (tt >> 2) * gridDim.x;
-    const uint64_t off = static_cast<uint64_t>(i) * 4u * E;
-    if (E == 1) {  // rows 8h .. 8h + 7
-#pragma unroll
-      for (uint32_t jj = 0; jj < 8; ++jj) {
-        const uint32_t j = 8 * half + jj;
-        if (j >= a.m) break;
-        uint32_t* p = reinterpret_cast<uint32_t*>(cur.at<E>(a, blk, a.k + j) + off);
-        *p = a.overwrite ? out[jj] : (out[jj] ^ *p);
-      }
-    } else if (E == 2) {  // rows 4h .. 4h + 3: bytes 0 and 1 of 4 elements, interleaved
-#pragma unroll
-      for (uint32_t jj = 0; jj < 4; ++jj) {
-        const uint32_t j = 4 * half + jj;
-        if (j >= a.m) break;
-        uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + off);
-        uint2 v = make_uint2(prmt(out[2 * jj], out[2 * jj + 1], 0x5140u), prmt(out[2 * jj], out[2 * jj + 1], 0x7362u));
-        if (!a.overwrite) {
-          const uint2 dd = *p;
-          v.x ^= dd.x;
-          v.y ^= dd.y;
-        }
-        *p = v;
-      }
-    } else {  // rows 2h, 2h + 1: 4 bytes of 4 elements, transposed
-#pragma unroll
-      for (uint32_t jj = 0; jj < 2; ++jj) {
-        const uint32_t j = 2 * half + jj;
-        if (j >= a.m) break;
-        uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + off);
-        const uint32_t* o = &out[4 * jj];
-        uint4 v = make_uint4(row_word4(o, 0), row_word4(o, 1), row_word4(o, 2), row_word4(o, 3));
-        if (!a.overwrite) {
-          const uint4 dd = *p;
-          v.x ^= dd.x;
-          v.y ^= dd.y;
-          v.z ^= dd.z;
-          v.w ^= dd.w;
-        }
-        *p = v;
-      }
-    }
-  }
-  return true;
 }
 
+// Epilogue warps (one per TMEM lane quarter q = output bits 32q .. 32q + 31,
+// i.e. output bytes 4q .. 4q + 3): per tile, read D 32 columns at a time; a
+// ballot of bit 7 over the warp's lanes is the column's 4 output bytes. Lane l
+// keeps columns 8l .. 8l + 7, releases D, then stores them.
 template <int E>
 __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, uint32_t d_base,
                                               volatile int* abort) {
-  uint32_t out[8];  // output bytes 8h .. 8h + 7 of this thread's 4 columns
-#pragma unroll
-  for (int x = 0; x < 8; ++x) out[x] = 0;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t q = warp & 3u;
+  const uint32_t lane_base = (32u * q) << 16;
+  const bool active = 4u * q < a.m * E;  // warp-uniform: this quarter holds output bytes
   StripeCursor cur;
   bool ok = true;
-  for (uint64_t t = 0; t < ntiles && ok; t += 4) {
-    ok = epilogue<E, 0>(a, S, d_base, t, out, abort, cur);
-    if (ok) ok = epilogue<E, 1>(a, S, d_base, t + 1, out, abort, cur);
-    if (ok) ok = epilogue<E, 2>(a, S, d_base, t + 2, out, abort, cur);
-    if (ok) ok = epilogue<E, 3>(a, S, d_base, t + 3, out, abort, cur);
+  for (uint64_t t = 0; t < ntiles; ++t) {
+    const uint32_t d = static_cast<uint32_t>(t % kDBufs);
+    if (!warp_wait(&S.dfull[d], static_cast<uint32_t>((t / kDBufs) & 1u), abort)) {
+      ok = false;
+      break;
+    }
+    tc_fence_after();
+    uint32_t w[8];
+#pragma unroll
+    for (int x = 0; x < 8; ++x) w[x] = 0;
+    if (active) {
+#pragma unroll
+      for (uint32_t ch = 0; ch < kTileCols / 32u; ch += 2) {
+        uint32_t r[64];
+        tmem_ld32(lane_base | (d_base + kTileCols * d + 32u * ch), r);
+        tmem_ld32(lane_base | (d_base + kTileCols * d + 32u * ch + 32u), r + 32);
+        tmem_wait_ld();
+#pragma unroll
+        for (uint32_t c = 0; c < 64; ++c) {
+          const uint32_t b = __ballot_sync(0xffffffffu, r[c] & 0x80u);
+          if (lane == 4u * ch + c / 8u) w[c % 8u] = b;
+        }
+      }
+    }
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.dempty[d]);  // a later product may overwrite D
+    if (active) {
+      const uint64_t blk = blockIdx.x + (t / 2u) * gridDim.x;
+      store_columns<E>(a, cur, blk, static_cast<uint32_t>(t % 2u) * kTileCols + 8u * lane, q, w);
+    }
   }
   if (!ok) {
     atomicExch(&g_gf2_err, 4);
@@ -498,54 +428,55 @@ __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint6
 
 template <int E>
 __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_constant__ Gf2Launch a) {
-  // dynamic shared memory: [B image (npad x K bytes)] [stages] [Smem]
   const uint32_t K = a.ngroups * 32u;
-  const uint32_t b_bytes = (a.npad * K + 1023u) & ~1023u;
+  const uint32_t a_bytes = a.ngroups * kABytesPerGroup;
   const uint32_t stage_bytes = (a.k * kCols * E + 127u) & ~127u;
-  uint8_t* bimg = g_smem;
-  uint8_t* stages = g_smem + b_bytes;
-  Smem& S = *reinterpret_cast<Smem*>(stages + kStages * stage_bytes);
+  uint8_t* aimg = g_smem;
+  uint8_t* slots = g_smem + a_bytes;
+  uint8_t* stages = slots + a.nslots * kSlotBytes;
+  Smem& S = *reinterpret_cast<Smem*>(stages + a.nstages * stage_bytes);
   volatile int* abort = &S.abort;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
 
-  // ---- B image: entry (n, kappa = 32 g + 4 b + r) = 2^(7 - b) where output
+  // ---- A image: entry (n, kappa = 32 g + 4 b + r) = 2^(7 - b) where output
   // bit n takes bit b of input byte 4 g + r; core matrix (kappa / 16, n / 8) at
-  // ((kappa / 16) * (npad / 8) + n / 8) * 128, row n % 8, byte kappa % 16
-  for (uint32_t i = threadIdx.x; i < a.npad * K / 16u; i += blockDim.x) {
-    const uint32_t core = i >> 3, row = i & 7u;
-    const uint32_t kc = core / (a.npad / 8u), n = (core % (a.npad / 8u)) * 8u + row;
+  // ((kappa / 16) * 16 + n / 8) * 128, row n % 8, byte kappa % 16 (M = 128
+  // rows, the rows past the m * E * 8 output bits zero)
+  for (uint32_t idx = threadIdx.x; idx < 128u * K / 16u; idx += blockDim.x) {
+    const uint32_t core = idx >> 3, row = idx & 7u;
+    const uint32_t kc = core >> 4, n = (core & 15u) * 8u + row;
     uint32_t w[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int qd = 0; qd < 4; ++qd) {
       uint32_t v = 0;
 #pragma unroll
       for (int x = 0; x < 4; ++x) {
-        const uint32_t kappa = kc * 16u + q * 4u + x;
+        const uint32_t kappa = kc * 16u + qd * 4u + x;
         const uint32_t g = kappa >> 5, b = (kappa >> 2) & 7u, r = kappa & 3u;
-        const uint32_t bit = (n < kMaxOutBits && g < kMaxInBits / 32u) ? (a.bits[n][g] >> (8u * r + b)) & 1u : 0u;
+        const uint32_t bit = (a.bits[n][g] >> (8u * r + b)) & 1u;
         v |= (bit << (7u - b)) << (8 * x);
       }
-      w[q] = v;
+      w[qd] = v;
     }
-    *reinterpret_cast<uint4*>(bimg + static_cast<size_t>(i) * 16u) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4*>(aimg + static_cast<size_t>(idx) * 16u) = make_uint4(w[0], w[1], w[2], w[3]);
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (uint32_t s = 0; s < a.nstages; ++s) {
       mbar_init(&S.full[s], 1);
       mbar_init(&S.empty[s], kExpandWarps);
     }
-    for (uint32_t s = 0; s < kSlots; ++s) {
-      mbar_init(&S.afull[s], kExpandWarps);
-      mbar_init(&S.aempty[s], 1);
+    for (uint32_t s = 0; s < a.nslots; ++s) {
+      mbar_init(&S.bfull[s], kExpandWarps);
+      mbar_init(&S.bempty[s], 1);
     }
     for (uint32_t d = 0; d < kDBufs; ++d) {
       mbar_init(&S.dfull[d], 1);
-      mbar_init(&S.dempty[d], kWorkerWarps - kExpandWarps);
+      mbar_init(&S.dempty[d], kEpilogueWarps);
     }
     S.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // generic-proxy writes of the B image become visible to the tensor cores
+  // generic-proxy writes of the A image become visible to the tensor cores
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   if (warp == kIssuerWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
@@ -556,25 +487,24 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tbase = S.tmem_base;
-  const uint32_t a_base = tbase;                        // kSlots slots x 32 columns
-  const uint32_t d_base = tbase + kSlots * kSlotCols;   // kDBufs buffers x 128 columns
+  const uint32_t d_base = S.tmem_base;  // kDBufs buffers x 256 columns
 
-  // blocks of this CTA: blockIdx.x, + gridDim.x, ...
+  // blocks of this CTA: blockIdx.x, + gridDim.x, ...; two tiles each
   const uint64_t nmine = a.nblk > blockIdx.x ? (a.nblk - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
-  const uint64_t ntiles = nmine * 4u;
+  const uint64_t ntiles = nmine * (kCols / kTileCols);
 
   if (warp == kProducerWarp) {
     // ---- producer: lane 0 arms the stage's barrier, every lane issues copies
     const uint32_t row_bytes = kCols * E;
     StripeCursor cur;
     uint64_t issued = 0;
-    for (uint64_t i = 0; i < nmine; ++i) {
-      const uint32_t s = static_cast<uint32_t>(i % kStages);
+    Ring st(a.nstages);
+    for (uint64_t i = 0; i < nmine; ++i, st.next()) {
+      const uint32_t s = st.i;
       int go = 1;
       if (lane == 0) {
         go = !*abort;
-        if (go && i >= kStages && !mbar_wait(&S.empty[s], static_cast<uint32_t>((i / kStages - 1) & 1u), abort)) {
+        if (go && st.reused && !mbar_wait(&S.empty[s], st.ph ^ 1u, abort)) {
           atomicExch(&g_gf2_err, 1);
           *abort = 1;
           go = 0;
@@ -590,49 +520,60 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
     }
     // copies still in flight must land before the CTA exits
     if (lane == 0)
-      for (uint64_t i = issued > kStages ? issued - kStages : 0; i < issued; ++i)
-        mbar_wait(&S.full[i % kStages], static_cast<uint32_t>((i / kStages) & 1u), abort, false);
+      for (uint64_t i = issued > a.nstages ? issued - a.nstages : 0; i < issued; ++i)
+        mbar_wait(&S.full[i % a.nstages], static_cast<uint32_t>((i / a.nstages) & 1u), abort, false);
   } else if (warp == kIssuerWarp) {
-    // ---- issuer: one thread issues every product, slot by slot
-    if (lane == 0) {
-      const uint32_t idesc = (2u << 4) | ((a.npad >> 3) << 17) | ((128u >> 4) << 24);  // s32 += u8 * u8, M = 128
-      const uint32_t bsm = smem_u32(bimg);
-      const uint32_t lbo = a.npad * 16u, sbo = 128u;
-      const uint32_t nq = (a.ngroups + 3u) / 4u;
-      uint64_t t = 0, qi = 0;
-      bool ok = true;
-      for (; t < ntiles && ok; ++t) {
-        const uint32_t d = static_cast<uint32_t>(t % kDBufs);
-        if (t >= kDBufs && !mbar_wait(&S.dempty[d], static_cast<uint32_t>((t / kDBufs - 1) & 1u), abort)) {
+    // ---- issuer: the whole warp walks the schedule, lane 0 issues (and commits)
+    const uint32_t idesc = (2u << 4) | ((kTileCols >> 3) << 17) | ((128u >> 4) << 24);  // s32 += u8*u8, M=128, N=256
+    const uint64_t a_desc0 = smem_desc(smem_u32(aimg), kABytesPerGroup / 2u, 128u);
+    const uint64_t b_desc0 = smem_desc(smem_u32(slots), kGroupBytes / 2u, 128u);
+    const uint32_t nq = (a.ngroups + kSlotGroups - 1) / kSlotGroups;
+    uint64_t t = 0;
+    Ring sl(a.nslots);
+    bool ok = true;
+    for (; t < ntiles && ok; ++t) {
+      const uint32_t d = static_cast<uint32_t>(t & 1u);
+      if (t >= kDBufs && !warp_wait(&S.dempty[d], static_cast<uint32_t>(((t >> 1) - 1u) & 1u), abort)) {
+        ok = false;
+        break;
+      }
+      const uint32_t dcol = d_base + kTileCols * d;
+      uint64_t ad = a_desc0;  // advanced by lane 0, the lane that issues
+      uint32_t acc = 0;       // the tile's first product overwrites D
+      for (uint32_t j = 0; j < nq; ++j, sl.next()) {
+        if (!warp_wait(&S.bfull[sl.i], sl.ph, abort)) {
           ok = false;
           break;
         }
-        for (uint32_t j = 0; j < nq; ++j, ++qi) {
-          const uint32_t slot = static_cast<uint32_t>(qi % kSlots);
-          if (!mbar_wait(&S.afull[slot], static_cast<uint32_t>((qi / kSlots) & 1u), abort)) {
-            ok = false;
-            break;
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t gn = min(kSlotGroups, a.ngroups - kSlotGroups * j);
+          uint64_t bd = b_desc0 + sl.i * (kSlotBytes >> 4);
+          for (uint32_t gg = 0; gg < gn; ++gg) {
+            mma_i8_ss(dcol, ad, bd, idesc, acc);
+            ad += kABytesPerGroup >> 4;
+            bd += kGroupBytes >> 4;
+            acc = 1;
           }
-          tc_fence_after();
-          const uint32_t gend = min(a.ngroups, 4u * j + 4u);
-          for (uint32_t g = 4u * j; g < gend; ++g)
-            mma_i8(d_base + 128u * d, a_base + kSlotCols * slot + 8u * (g - 4u * j),
-                   smem_desc(bsm + g * 2u * a.npad * 16u, lbo, sbo), idesc, g > 0);
-          mma_commit(&S.aempty[slot]);  // this slot may be refilled once its products are done
+          mma_commit(&S.bempty[sl.i]);  // the slot may be refilled once its products are done
         }
-        if (!ok) break;
-        mma_commit(&S.dfull[d]);
+        __syncwarp();
       }
-      if (!ok) {
-        atomicExch(&g_gf2_err, 2);
-        *abort = 1;
-      }
-      // the last products must finish before TMEM is freed
+      if (!ok) break;
+      if (lane == 0) mma_commit(&S.dfull[d]);
+      __syncwarp();
+    }
+    if (!ok) {
+      if (lane == 0) atomicExch(&g_gf2_err, 2);
+      *abort = 1;
+    }
+    // the last products must finish before TMEM is freed
+    if (lane == 0)
       for (uint64_t u = t > kDBufs ? t - kDBufs : 0; u < t; ++u)
         mbar_wait(&S.dfull[u % kDBufs], static_cast<uint32_t>((u / kDBufs) & 1u), abort, false);
-    }
+    __syncwarp();
   } else if (warp < kExpandWarps) {
-    expander_loop<E>(a, S, stages, stage_bytes, nmine, a_base, abort);
+    expander_loop<E>(a, S, stages, stage_bytes, a.nstages, smem_u32(slots), a.nslots, nmine, abort);
   } else {
     epilogue_loop<E>(a, S, ntiles, d_base, abort);
   }
@@ -640,7 +581,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
   __syncthreads();
   tc_fence_after();
   if (warp == kIssuerWarp)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(d_base), "r"(kTmemCols) : "memory");
 }
 
 }  // namespace
@@ -686,13 +627,22 @@ cudaError_t launch_common(Gf2Launch& a, int field, size_t k, size_t m, const uin
   a.m = static_cast<uint32_t>(m);
   a.E = static_cast<uint32_t>(E);
   a.ngroups = static_cast<uint32_t>((k * E + 3) / 4);
-  a.npad = static_cast<uint32_t>((m * E * 8 + 15) / 16 * 16);
   a.overwrite = overwrite ? 1u : 0u;
   std::memcpy(a.bits, bits, sizeof a.bits);
-  const uint32_t K = a.ngroups * 32u;
-  const uint32_t b_bytes = (a.npad * K + 1023u) & ~1023u;
-  const uint32_t stage_bytes = (a.k * kCols * E + 127u) & ~127u;
-  const int smem = static_cast<int>(b_bytes + kStages * stage_bytes + sizeof(Smem));
+  // shared memory: the A image, then at least 2 B slots and 2 source stages;
+  // what is left buys a third slot, then up to kMaxStages stages, then up to
+  // kMaxSlots slots
+  const size_t a_bytes = static_cast<size_t>(a.ngroups) * kABytesPerGroup;
+  const size_t stage_bytes = (static_cast<size_t>(k) * kCols * E + 127u) & ~static_cast<size_t>(127u);
+  uint32_t nst = 2, nsl = 2;
+  const auto total = [&](uint32_t st, uint32_t sl) { return a_bytes + sl * kSlotBytes + st * stage_bytes + sizeof(Smem); };
+  if (nsl < 3 && total(nst, 3) <= kMaxLaunchSmem) nsl = 3;
+  while (nst < kMaxStages && total(nst + 1, nsl) <= kMaxLaunchSmem) ++nst;
+  while (nsl < kMaxSlots && total(nst, nsl + 1) <= kMaxLaunchSmem) ++nsl;
+  if (total(nst, nsl) > kMaxLaunchSmem) return cudaErrorInvalidValue;
+  a.nstages = nst;
+  a.nslots = nsl;
+  const int smem = static_cast<int>(total(nst, nsl));
   const void* fn = E == 1 ? reinterpret_cast<const void*>(gf2mma_kernel<1>)
                           : (E == 2 ? reinterpret_cast<const void*>(gf2mma_kernel<2>)
                                     : reinterpret_cast<const void*>(gf2mma_kernel<4>));
