@@ -30,15 +30,16 @@
 //     column's input bytes from the stage and write its expanded input bits
 //     into a ring of B slots in shared memory (4 input groups, K = 128, per
 //     slot), each slot handed to the issuer through an mbarrier;
-//   * warp 13 (issuer): allocates TMEM (two D buffers of 256 columns),
+//   * warp 17 (issuer): allocates TMEM (two D buffers of 256 columns),
 //     issues the K/32 products of a tile from one lane, A and B
 //     both from shared memory, commits each slot back to the expanders once
 //     its products are done and the tile to the epilogue;
-//   * warps 8..11 (epilogue, one per TMEM lane quarter = 4 output bytes):
-//     read D back 32 columns at a time (tcgen05.ld), turn bit 7 of the 32
-//     lanes into the column's 4 output bytes with one ballot, release D and
-//     store 8 consecutive columns per lane;
-//   * warp 12 (producer): see above, every lane issuing copies.
+//   * warps 8..15 (epilogue, two per TMEM lane quarter = 4 output bytes,
+//     one per half of the tile's columns): read D back 32 columns at a time
+//     (tcgen05.ld), turn bit 7 of the 32 lanes into the column's 4 output
+//     bytes with one ballot, release D and store 4 consecutive columns per
+//     lane;
+//   * warp 16 (producer): see above, every lane issuing copies.
 // Every mbarrier wait is bounded: a wait that runs out sets the error word,
 // stops the CTA's loops, waits (bounded) for its own copies and products in
 // flight and frees TMEM before returning.
@@ -58,10 +59,10 @@ namespace fgfc {
 namespace {
 
 constexpr int kExpandWarps = 8;                        // warps 0 .. 7: expand inputs into B slots
-constexpr int kEpilogueWarps = 4;                      // warps 8 .. 11: read D back, one per lane quarter
+constexpr int kEpilogueWarps = 8;                      // warps 8 .. 15: read D back, two per lane quarter
 constexpr int kProducerWarp = kExpandWarps + kEpilogueWarps;  // bulk copies of source blocks
 constexpr int kIssuerWarp = kProducerWarp + 1;         // TMEM allocation and the products
-constexpr int kMmaThreads = (kIssuerWarp + 1) * 32;    // 448
+constexpr int kMmaThreads = (kIssuerWarp + 1) * 32;    // 576
 constexpr uint32_t kCols = 512;        // element columns per block (2 tiles of 256)
 constexpr uint32_t kMaxInBits = 512;   // K
 constexpr uint32_t kMaxOutBits = 128;  // M
@@ -129,14 +130,21 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 // Wait bounded in time (every wait of a correct run lasts microseconds);
 // false when it ran out. With `honor_abort` it also gives up once another
-// role has aborted (the drain waits before exit do not).
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, bool honor_abort = true) {
+// role has aborted (the drain waits before exit do not). Between tries the
+// thread sleeps (16 ns, doubling up to `max_sleep_ns`): back-to-back
+// try_wait polling by a dozen waiting warps takes so much of the shared
+// memory pipe that the tensor cores' operand reads slow several-fold.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, bool honor_abort = true,
+                                          uint32_t max_sleep_ns = 256) {
   if (mbar_try(b, parity)) return true;
   const uint64_t t0 = global_ns();
   const uint64_t limit = honor_abort ? kWaitNs : kDrainNs;
+  uint32_t sleep_ns = 16;
   for (uint32_t i = 1;; ++i) {
+    __nanosleep(sleep_ns);
     if (mbar_try(b, parity)) return true;
-    if ((i & 255u) == 0) {
+    sleep_ns = min(2u * sleep_ns, max_sleep_ns);
+    if ((i & 15u) == 0) {
       if (honor_abort && *abort) return false;
       if (global_ns() - t0 > limit) return false;
     }
@@ -145,8 +153,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
 
 // The same wait by every lane of a warp, with a warp-uniform result (the
 // tcgen05 .sync.aligned instructions that follow need the whole warp).
-__device__ __forceinline__ bool warp_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
-  const bool ok = mbar_wait(b, parity, abort);
+__device__ __forceinline__ bool warp_wait(uint64_t* b, uint32_t parity, volatile int* abort,
+                                          uint32_t max_sleep_ns = 256) {
+  const bool ok = mbar_wait(b, parity, abort, true, max_sleep_ns);
   return __all_sync(0xffffffffu, ok);
 }
 
@@ -297,7 +306,7 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
     for (uint32_t T = 0; T < kCols / kTileCols && ok; ++T) {
       const uint32_t col = T * kTileCols + i;
       for (uint32_t j = 0; j < nq; ++j, sl.next()) {
-        if (sl.reused && !warp_wait(&S.bempty[sl.i], sl.ph ^ 1u, abort)) {
+        if (sl.reused && !warp_wait(&S.bempty[sl.i], sl.ph ^ 1u, abort, 64)) {
           ok = false;
           break;
         }
@@ -326,33 +335,32 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
   }
 }
 
-// Output words of 8 consecutive columns (w[x] = output bytes 4q .. 4q + 3 of
-// column col0 + x, byte i = output byte 4q + i) into the rows they belong to.
+// Output words of 4 consecutive columns (w[x] = output bytes 4q .. 4q + 3 of
+// column colb + x, byte i = output byte 4q + i) into the rows they belong to.
 template <int E>
 __device__ __forceinline__ void store_columns(const Gf2Launch& a, StripeCursor& cur, uint64_t blk, uint32_t colb,
-                                              uint32_t q, const uint32_t (&w)[8]) {
-  if (E == 4) {  // row q: 8 elements
+                                              uint32_t q, const uint32_t (&w)[4]) {
+  if (E == 4) {  // row q: 4 elements
     if (q >= a.m) return;
     uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + q) + colb * 4u);
-    uint4 v0 = make_uint4(w[0], w[1], w[2], w[3]), v1 = make_uint4(w[4], w[5], w[6], w[7]);
+    uint4 v = make_uint4(w[0], w[1], w[2], w[3]);
     if (!a.overwrite) {
-      const uint4 d0 = p[0], d1 = p[1];
-      v0.x ^= d0.x; v0.y ^= d0.y; v0.z ^= d0.z; v0.w ^= d0.w;
-      v1.x ^= d1.x; v1.y ^= d1.y; v1.z ^= d1.z; v1.w ^= d1.w;
+      const uint4 d = *p;
+      v.x ^= d.x; v.y ^= d.y; v.z ^= d.z; v.w ^= d.w;
     }
-    p[0] = v0;
-    p[1] = v1;
+    *p = v;
   } else if (E == 2) {  // rows 2q (low halves) and 2q + 1 (high halves)
 #pragma unroll
     for (uint32_t h = 0; h < 2; ++h) {
       const uint32_t j = 2u * q + h;
       if (j >= a.m) break;
       const uint32_t sel = h ? 0x7632u : 0x5410u;
-      uint4 v = make_uint4(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel), prmt(w[4], w[5], sel), prmt(w[6], w[7], sel));
-      uint4* p = reinterpret_cast<uint4*>(cur.at<E>(a, blk, a.k + j) + colb * 2u);
+      uint2 v = make_uint2(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel));
+      uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + colb * 2u);
       if (!a.overwrite) {
-        const uint4 d = *p;
-        v.x ^= d.x; v.y ^= d.y; v.z ^= d.z; v.w ^= d.w;
+        const uint2 d = *p;
+        v.x ^= d.x;
+        v.y ^= d.y;
       }
       *p = v;
     }
@@ -362,53 +370,49 @@ __device__ __forceinline__ void store_columns(const Gf2Launch& a, StripeCursor& 
       const uint32_t j = 4u * q + r;
       if (j >= a.m) break;
       const uint32_t sel = r | ((4u + r) << 4);
-      uint2 v = make_uint2(prmt(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel), 0x5410u),
-                           prmt(prmt(w[4], w[5], sel), prmt(w[6], w[7], sel), 0x5410u));
-      uint2* p = reinterpret_cast<uint2*>(cur.at<E>(a, blk, a.k + j) + colb);
-      if (!a.overwrite) {
-        const uint2 d = *p;
-        v.x ^= d.x;
-        v.y ^= d.y;
-      }
+      uint32_t v = prmt(prmt(w[0], w[1], sel), prmt(w[2], w[3], sel), 0x5410u);
+      uint32_t* p = reinterpret_cast<uint32_t*>(cur.at<E>(a, blk, a.k + j) + colb);
+      if (!a.overwrite) v ^= *p;
       *p = v;
     }
   }
 }
 
-// Epilogue warps (one per TMEM lane quarter q = output bits 32q .. 32q + 31,
-// i.e. output bytes 4q .. 4q + 3): per tile, read D 32 columns at a time; a
-// ballot of bit 7 over the warp's lanes is the column's 4 output bytes. Lane l
-// keeps columns 8l .. 8l + 7, releases D, then stores them.
+// Epilogue warps 8 .. 15: warp e reads TMEM lane quarter q = e % 4 (output
+// bits 32q .. 32q + 31, i.e. output bytes 4q .. 4q + 3) for the half
+// h = (e - 8) / 4 of the tile's columns (128 columns), 32 columns per load.
+// A ballot of bit 7 over the warp's lanes is one column's 4 output bytes;
+// lane l keeps columns 4l .. 4l + 3 of the half, releases D, then stores.
 template <int E>
 __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, uint32_t d_base,
                                               volatile int* abort) {
+  constexpr uint32_t kHalfCols = kTileCols / 2u;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const uint32_t q = warp & 3u;
+  const uint32_t q = warp & 3u, half = (warp - kExpandWarps) >> 2;
   const uint32_t lane_base = (32u * q) << 16;
   const bool active = 4u * q < a.m * E;  // warp-uniform: this quarter holds output bytes
   StripeCursor cur;
   bool ok = true;
   for (uint64_t t = 0; t < ntiles; ++t) {
-    const uint32_t d = static_cast<uint32_t>(t % kDBufs);
-    if (!warp_wait(&S.dfull[d], static_cast<uint32_t>((t / kDBufs) & 1u), abort)) {
+    const uint32_t d = static_cast<uint32_t>(t & 1u);
+    if (!warp_wait(&S.dfull[d], static_cast<uint32_t>((t >> 1) & 1u), abort, 128)) {
       ok = false;
       break;
     }
     tc_fence_after();
-    uint32_t w[8];
-#pragma unroll
-    for (int x = 0; x < 8; ++x) w[x] = 0;
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
     if (active) {
+      const uint32_t col0 = d_base + kTileCols * d + kHalfCols * half;
 #pragma unroll
-      for (uint32_t ch = 0; ch < kTileCols / 32u; ch += 2) {
+      for (uint32_t ch = 0; ch < kHalfCols / 32u; ch += 2) {
         uint32_t r[64];
-        tmem_ld32(lane_base | (d_base + kTileCols * d + 32u * ch), r);
-        tmem_ld32(lane_base | (d_base + kTileCols * d + 32u * ch + 32u), r + 32);
+        tmem_ld32(lane_base | (col0 + 32u * ch), r);
+        tmem_ld32(lane_base | (col0 + 32u * ch + 32u), r + 32);
         tmem_wait_ld();
 #pragma unroll
         for (uint32_t c = 0; c < 64; ++c) {
           const uint32_t b = __ballot_sync(0xffffffffu, r[c] & 0x80u);
-          if (lane == 4u * ch + c / 8u) w[c % 8u] = b;
+          if (lane == 8u * ch + c / 4u) w[c % 4u] = b;
         }
       }
     }
@@ -416,8 +420,8 @@ __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint6
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.dempty[d]);  // a later product may overwrite D
     if (active) {
-      const uint64_t blk = blockIdx.x + (t / 2u) * gridDim.x;
-      store_columns<E>(a, cur, blk, static_cast<uint32_t>(t % 2u) * kTileCols + 8u * lane, q, w);
+      const uint64_t blk = blockIdx.x + (t >> 1) * gridDim.x;
+      store_columns<E>(a, cur, blk, static_cast<uint32_t>(t & 1u) * kTileCols + kHalfCols * half + 4u * lane, q, w);
     }
   }
   if (!ok) {
@@ -533,7 +537,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
     bool ok = true;
     for (; t < ntiles && ok; ++t) {
       const uint32_t d = static_cast<uint32_t>(t & 1u);
-      if (t >= kDBufs && !warp_wait(&S.dempty[d], static_cast<uint32_t>(((t >> 1) - 1u) & 1u), abort)) {
+      if (t >= kDBufs && !warp_wait(&S.dempty[d], static_cast<uint32_t>(((t >> 1) - 1u) & 1u), abort, 32)) {
         ok = false;
         break;
       }
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
       uint64_t ad = a_desc0;  // advanced by lane 0, the lane that issues
       uint32_t acc = 0;       // the tile's first product overwrites D
       for (uint32_t j = 0; j < nq; ++j, sl.next()) {
-        if (!warp_wait(&S.bfull[sl.i], sl.ph, abort)) {
+        if (!warp_wait(&S.bfull[sl.i], sl.ph, abort, 32)) {
           ok = false;
           break;
         }
