@@ -36,9 +36,9 @@
 //     its products are done and the tile to the epilogue;
 //   * warps 8..15 (epilogue, two per TMEM lane quarter = 4 output bytes,
 //     one per half of the tile's columns): read D back 32 columns at a time
-//     (tcgen05.ld), turn bit 7 of the 32 lanes into the column's 4 output
-//     bytes with one ballot, release D and store 4 consecutive columns per
-//     lane;
+//     (tcgen05.ld), pack bit 7 of each lane's 32 accumulators into a word,
+//     transpose the warp's 32 words (5 shuffle steps) so that lane c holds
+//     column c's 4 output bytes, release D and store;
 //   * warp 16 (producer): see above, every lane issuing copies.
 // Every mbarrier wait is bounded: a wait that runs out sets the error word,
 // stops the CTA's loops, waits (bounded) for its own copies and products in
@@ -335,6 +335,30 @@ __device__ __forceinline__ void expander_loop(const Gf2Launch& a, Smem& S, const
   }
 }
 
+// Bits 7 of 8 accumulators as one byte (bit o = bit 7 of r[o]) in bits 24..31.
+// Every accumulator is 128 * (number of 1 products), so byte 0 of each holds
+// bit 7 alone: PRMT gathers the 8 low bytes into two words, and one
+// multiply-add moves bit 7 of byte i to bit 24 + i (p03) or 28 + i (p47);
+// the shifted copies never land on the same bit.
+__device__ __forceinline__ uint32_t pack_byte(const uint32_t* r) {
+  const uint32_t p03 = prmt(prmt(r[0], r[1], 0x0040u), prmt(r[2], r[3], 0x0040u), 0x5410u);
+  const uint32_t p47 = prmt(prmt(r[4], r[5], 0x0040u), prmt(r[6], r[7], 0x0040u), 0x5410u);
+  return (p03 >> 4) * 0x00204081u + p47 * 0x00204081u;
+}
+
+// 32 x 32 bit-matrix transpose across a warp: on entry bit c of lane l's word
+// is M[l][c], on return bit c of lane l's word is M[c][l]. Five exchange
+// steps swap the off-diagonal j x j blocks of every 2j x 2j block.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (uint32_t j = 16; j >= 1; j >>= 1) {
+    const uint32_t lo = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu : j == 2 ? 0x33333333u : 0x55555555u;
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~lo) | ((y >> j) & lo)) : ((x & lo) | ((y << j) & ~lo));
+  }
+  return x;
+}
+
 // Output words of 4 consecutive columns (w[x] = output bytes 4q .. 4q + 3 of
 // column colb + x, byte i = output byte 4q + i) into the rows they belong to.
 template <int E>
@@ -381,12 +405,16 @@ __device__ __forceinline__ void store_columns(const Gf2Launch& a, StripeCursor& 
 // Epilogue warps 8 .. 15: warp e reads TMEM lane quarter q = e % 4 (output
 // bits 32q .. 32q + 31, i.e. output bytes 4q .. 4q + 3) for the half
 // h = (e - 8) / 4 of the tile's columns (128 columns), 32 columns per load.
-// A ballot of bit 7 over the warp's lanes is one column's 4 output bytes;
-// lane l keeps columns 4l .. 4l + 3 of the half, releases D, then stores.
+// Lane l packs bit 7 of its 32 accumulators (output bit 32q + l of 32
+// columns) into one word; a warp transpose of those 32 words gives lane c the
+// 4 output bytes of column c. D is released once the half is read; 16
+// shuffles then hand lane l the 4 consecutive columns 4l .. 4l + 3 it stores.
 template <int E>
 __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint64_t ntiles, uint32_t d_base,
                                               volatile int* abort) {
   constexpr uint32_t kHalfCols = kTileCols / 2u;
+  constexpr uint32_t kChunks = kHalfCols / 32u;
+  static_assert(kChunks == 4, "the regroup below hands each lane 4 columns of one chunk");
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t q = warp & 3u, half = (warp - kExpandWarps) >> 2;
   const uint32_t lane_base = (32u * q) << 16;
@@ -400,28 +428,38 @@ __device__ __forceinline__ void epilogue_loop(const Gf2Launch& a, Smem& S, uint6
       break;
     }
     tc_fence_after();
-    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    uint32_t w[kChunks];
+#pragma unroll
+    for (uint32_t ch = 0; ch < kChunks; ++ch) w[ch] = 0;
     if (active) {
       const uint32_t col0 = d_base + kTileCols * d + kHalfCols * half;
 #pragma unroll
-      for (uint32_t ch = 0; ch < kHalfCols / 32u; ch += 2) {
-        uint32_t r[64];
+      for (uint32_t ch = 0; ch < kChunks; ++ch) {
+        uint32_t r[32];
         tmem_ld32(lane_base | (col0 + 32u * ch), r);
-        tmem_ld32(lane_base | (col0 + 32u * ch + 32u), r + 32);
         tmem_wait_ld();
-#pragma unroll
-        for (uint32_t c = 0; c < 64; ++c) {
-          const uint32_t b = __ballot_sync(0xffffffffu, r[c] & 0x80u);
-          if (lane == 8u * ch + c / 4u) w[c % 4u] = b;
-        }
+        const uint32_t b0 = pack_byte(r), b1 = pack_byte(r + 8), b2 = pack_byte(r + 16), b3 = pack_byte(r + 24);
+        w[ch] = prmt(prmt(b0, b1, 0x0073u), prmt(b2, b3, 0x0073u), 0x5410u);  // bit c = column c
       }
     }
     tc_fence_before();
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.dempty[d]);  // a later product may overwrite D
     if (active) {
+      // lane c of chunk ch holds column 32 ch + c; regroup so that lane l
+      // holds columns 4l .. 4l + 3 (chunk l / 8, lanes 4 (l % 8) + x)
+      uint32_t o[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (uint32_t ch = 0; ch < kChunks; ++ch) {
+        const uint32_t tw = warp_transpose32(w[ch], lane);
+#pragma unroll
+        for (uint32_t x = 0; x < 4; ++x) {
+          const uint32_t v = __shfl_sync(0xffffffffu, tw, 4u * (lane & 7u) + x);
+          if ((lane >> 3) == ch) o[x] = v;
+        }
+      }
       const uint64_t blk = blockIdx.x + (t >> 1) * gridDim.x;
-      store_columns<E>(a, cur, blk, static_cast<uint32_t>(t & 1u) * kTileCols + kHalfCols * half + 4u * lane, q, w);
+      store_columns<E>(a, cur, blk, static_cast<uint32_t>(t & 1u) * kTileCols + kHalfCols * half + 4u * lane, q, o);
     }
   }
   if (!ok) {

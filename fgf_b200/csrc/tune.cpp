@@ -78,15 +78,18 @@ int forced_locked() {
   return g_force;
 }
 
-// Built-in rules (B200 measurements): byte tables reach the HBM roofline for
-// their shapes once a row is long enough to amortise the 1.5 us table fill;
-// the tensor-core contraction wins once the arithmetic per source byte
-// (m * E * 8 output bits) outgrows what shared-memory lookups sustain.
+// Built-in rules (B200 measurements of dot_product_matrix over 1 and 4 MiB
+// rows, every field, k * E in {4 .. 64} bytes, m * E in {1 .. 16} bytes):
+// byte tables reach the HBM roofline for their shapes once a row is long
+// enough to amortise the 1.5 us table fill; the tensor-core contraction
+// wins where a column carries the most output it takes (m * E = 16 bytes)
+// from at least 32 input bytes (Gf8 RS(64,16), Gf16 RS(16..32,8), Gf32
+// RS(8..16,4): 1.1 - 1.6x the split-nibble kernel, whose lookups per output
+// bit cost the most there).
 int builtin_choice(int field, size_t k, size_t m, size_t len) {
-  const int E = field_bytes(field);
+  const size_t E = static_cast<size_t>(field_bytes(field));
   if (kernel_usable(FGFC_KERNEL_BYTE, field, k, m) && len >= (4u << 20)) return FGFC_KERNEL_BYTE;
-  if (kernel_usable(FGFC_KERNEL_GF2MMA, field, k, m) && len >= (256u << 10) &&
-      static_cast<size_t>(E) * m >= 6)
+  if (kernel_usable(FGFC_KERNEL_GF2MMA, field, k, m) && len >= (1u << 20) && E * m >= 16 && E * k >= 32)
     return FGFC_KERNEL_GF2MMA;
   return FGFC_KERNEL_NIBBLE;
 }
