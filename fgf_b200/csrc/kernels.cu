@@ -383,53 +383,109 @@ __global__ void xor_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict_
   }
 }
 
-__constant__ uint8_t c_exp[2][512];
-__constant__ uint8_t c_log[2][256];
-// __constant__ memory is per device: the tables are uploaded once per device.
+// Per-device caches (SM count) are arrays indexed by device ordinal.
 constexpr int kMaxDevices = 64;
-std::atomic<bool> g_const_ready[kMaxDevices];
-std::mutex g_const_mu;
 
-__device__ __forceinline__ uint8_t emul(const uint8_t* ex, const uint8_t* lg, uint8_t x, uint8_t y) {
-  return (x && y) ? ex[lg[x] + lg[y]] : 0;
+// ---- mul_elementwise: products of two vectors, without tables.
+//
+// GF(2^8) products of 4 byte lanes of a 32-bit word at once by shifts and
+// XORs: x * y = XOR over the set bits b of y of x * 2^b, where x * 2 is the
+// byte-wise shift left reduced by the field polynomial in the lanes whose
+// bit 7 falls out. A permute whose selector nibble is 8 + i copies the top
+// bit of byte i over the whole byte, so each byte mask costs one PRMT.
+// Gf16 and Gf32 use their tower identities over these byte products:
+//   (a + b u)(c + d u) = (ac + 0x20 bd) + ((a + b)(c + d) + ac) u      (Gf16)
+//   (A + B v)(C + D v) = (AC + 0x2000 BD) + ((A + B)(C + D) + AC) v   (Gf32)
+// (src/field/gf16.rs:54-60, src/field/gf32.rs:36-42). No lookups means no
+// shared-memory bank conflicts; the kernel is bound by HBM for Gf8.
+
+__device__ __forceinline__ uint32_t prmt_sign(uint32_t a, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, 0, %2;" : "=r"(d) : "r"(a), "r"(sel));
+  return d;
 }
 
+// 4 byte lanes times 2, reduced by the polynomial whose low byte is R.
+template <uint32_t R>
+__device__ __forceinline__ uint32_t xtime4(uint32_t x) {
+  return ((x & 0x7F7F7F7Fu) << 1) ^ (prmt_sign(x, 0xBA98u) & (R * 0x01010101u));
+}
+
+// 4 independent GF(2^8) products (byte lane i of x times byte lane i of y).
+template <uint32_t R>
+__device__ __forceinline__ uint32_t gmul4(uint32_t x, uint32_t y) {
+  uint32_t acc = 0;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    acc ^= x & prmt_sign(y << (7 - b), 0xBA98u);  // lanes whose bit b of y is set
+    if (b < 7) x = xtime4<R>(x);
+  }
+  return acc;
+}
+
+// Two Gf16 products per word: elements [a, b] in bytes 0-1 and 2-3.
+__device__ __forceinline__ uint32_t gmul16x2(uint32_t x, uint32_t y) {
+  const uint32_t p = gmul4<0x1Bu>(x, y);                                   // [ac, bd, ...]
+  const uint32_t q = gmul4<0x1Bu>(x ^ prmt(x, 0u, 0x2301u), y ^ prmt(y, 0u, 0x2301u));  // [(a+b)(c+d), ...]
+  uint32_t c = p;                                                          // 0x20 * p: five doublings
+#pragma unroll
+  for (int i = 0; i < 5; ++i) c = xtime4<0x1Bu>(c);
+  // [ac + 0x20 bd, (a+b)(c+d) + ac] per element
+  return prmt(p, p, 0x2200u) ^ prmt(c, q, 0x7351u);
+}
+
+// One Gf32 product per word: [A, B] as Gf16 halves.
+__device__ __forceinline__ uint32_t gmul32(uint32_t x, uint32_t y) {
+  const uint32_t p = gmul16x2(x, y);                                       // [AC, BD]
+  const uint32_t q = gmul16x2(x ^ prmt(x, 0u, 0x1032u), y ^ prmt(y, 0u, 0x1032u));  // [(A+B)(C+D), ..]
+  const uint32_t c = gmul16x2(p, 0x20002000u);                            // [0x2000 AC, 0x2000 BD]
+  return prmt(p ^ (c >> 16), q ^ p, 0x5410u);                             // [AC + 0x2000 BD, (A+B)(C+D) + AC]
+}
+
+// One word of 32-bit lanes holding 4 bytes of each vector (a whole number of
+// elements: 4 Gf8, 2 Gf16, 1 Gf32).
 template <int F>
-__global__ void elementwise_kernel(uint8_t* dst, const uint8_t* a, const uint8_t* b, uint64_t nelem) {
-  __shared__ uint8_t ex[512];
-  __shared__ uint8_t lg[256];
-  constexpr int sel = (F == kGf8D) ? 1 : 0;
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) ex[i] = c_exp[sel][i];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) lg[i] = c_log[sel][i];
-  __syncthreads();
+__device__ __forceinline__ uint32_t emul_word(uint32_t x, uint32_t y) {
+  if (F == kGf8B) return gmul4<0x1Bu>(x, y);
+  if (F == kGf8D) return gmul4<0x1Du>(x, y);
+  if (F == kGf16) return gmul16x2(x, y);
+  return gmul32(x, y);
+}
+
+// Vector path: dst, a and b share their offset within 16 bytes and the first
+// `head` bytes (a whole number of elements) run through the scalar path, so
+// the body is 16-byte loads and stores; `nvec` 16-byte vectors follow.
+// Scalar path (head, tail, or every element when the offsets differ): one
+// element per thread step, its bytes gathered into the low lanes of a word.
+template <int F>
+__global__ void elementwise_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ a,
+                                   const uint8_t* __restrict__ b, uint64_t len, uint64_t head, uint64_t nvec) {
+  constexpr int E = (F == kGf16) ? 2 : (F == kGf32 ? 4 : 1);
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem;
-       i += stride) {
-    if (F == kGf8B || F == kGf8D) {
-      dst[i] = emul(ex, lg, a[i], b[i]);
-    } else if (F == kGf16) {
-      const uint8_t x0 = a[2 * i], x1 = a[2 * i + 1], y0 = b[2 * i], y1 = b[2 * i + 1];
-      const uint8_t ac = emul(ex, lg, x0, y0), bd = emul(ex, lg, x1, y1);
-      dst[2 * i] = ac ^ emul(ex, lg, 0x20, bd);
-      dst[2 * i + 1] = emul(ex, lg, x0 ^ x1, y0 ^ y1) ^ ac;
-    } else {
-      auto m16 = [&](uint16_t x, uint16_t y) -> uint16_t {
-        const uint8_t p0 = x & 0xFF, p1 = x >> 8, q0 = y & 0xFF, q1 = y >> 8;
-        const uint8_t ac = emul(ex, lg, p0, q0), bd = emul(ex, lg, p1, q1);
-        const uint8_t lo = ac ^ emul(ex, lg, 0x20, bd);
-        const uint8_t hi = emul(ex, lg, p0 ^ p1, q0 ^ q1) ^ ac;
-        return static_cast<uint16_t>(lo | (hi << 8));
-      };
-      const uint16_t xa = a[4 * i] | (a[4 * i + 1] << 8), xb = a[4 * i + 2] | (a[4 * i + 3] << 8);
-      const uint16_t ya = b[4 * i] | (b[4 * i + 1] << 8), yb = b[4 * i + 2] | (b[4 * i + 3] << 8);
-      const uint16_t ac = m16(xa, ya), bd = m16(xb, yb);
-      const uint16_t lo = ac ^ m16(0x2000, bd);
-      const uint16_t hi = m16(xa ^ xb, ya ^ yb) ^ ac;
-      dst[4 * i] = lo & 0xFF;
-      dst[4 * i + 1] = lo >> 8;
-      dst[4 * i + 2] = hi & 0xFF;
-      dst[4 * i + 3] = hi >> 8;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (uint64_t v = tid; v < nvec; v += stride) {
+    const uint64_t o = head + 16 * v;
+    const uint4 x = ldg16(a + o), y = ldg16(b + o);
+    uint4 r;
+    r.x = emul_word<F>(x.x, y.x);
+    r.y = emul_word<F>(x.y, y.y);
+    r.z = emul_word<F>(x.z, y.z);
+    r.w = emul_word<F>(x.w, y.w);
+    *reinterpret_cast<uint4*>(dst + o) = r;
+  }
+  const uint64_t tail0 = head + 16 * nvec;
+  const uint64_t nscalar = (head + (len - tail0)) / E;
+  for (uint64_t i = tid; i < nscalar; i += stride) {
+    const uint64_t o = i * E < head ? i * E : tail0 + (i * E - head);
+    uint32_t x = 0, y = 0;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      x |= static_cast<uint32_t>(a[o + k]) << (8 * k);
+      y |= static_cast<uint32_t>(b[o + k]) << (8 * k);
     }
+    const uint32_t r = emul_word<F>(x, y);
+#pragma unroll
+    for (int k = 0; k < E; ++k) dst[o + k] = static_cast<uint8_t>(r >> (8 * k));
   }
 }
 
@@ -504,32 +560,25 @@ cudaError_t launch_xor(uint8_t* dst, const uint8_t* src, uint64_t len, cudaStrea
 cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
                                uint64_t len, cudaStream_t s) {
   if (!len) return cudaSuccess;
-  int dev = 0;
-  cudaError_t de = cudaGetDevice(&dev);
-  if (de != cudaSuccess) return de;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_const_ready[dev].load(std::memory_order_acquire)) {
-    std::lock_guard<std::mutex> lk(g_const_mu);
-    uint8_t ex[2][512], lg[2][256];
-    const Gf8Log* t[2] = {&gf8b_tab(), &gf8d_tab()};
-    for (int w = 0; w < 2; ++w) {
-      for (int i = 0; i < 512; ++i) ex[w][i] = t[w]->exp[i];
-      for (int i = 0; i < 256; ++i) lg[w][i] = t[w]->log[i];
+  const int E = field_bytes(field);
+  if (E <= 0 || len % E) return cudaErrorInvalidValue;
+  const uint64_t ad = reinterpret_cast<uintptr_t>(dst) & 15;
+  uint64_t head = len, nvec = 0;
+  if (ad == (reinterpret_cast<uintptr_t>(a) & 15) && ad == (reinterpret_cast<uintptr_t>(b) & 15)) {
+    const uint64_t h = (16 - ad) & 15;
+    if (h % E == 0 && h <= len) {
+      head = h;
+      nvec = (len - h) / 16;
     }
-    cudaError_t e = cudaMemcpyToSymbol(c_exp, ex, sizeof(ex));
-    if (e != cudaSuccess) return e;
-    e = cudaMemcpyToSymbol(c_log, lg, sizeof(lg));
-    if (e != cudaSuccess) return e;
-    g_const_ready[dev].store(true, std::memory_order_release);
   }
-  const uint64_t nelem = len / field_bytes(field);
-  uint64_t want = (nelem + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
+  const uint64_t work = nvec + (len - 16 * nvec) / E;
+  uint64_t want = (work + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
   const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
   switch (field) {
-    case kGf8B: elementwise_kernel<kGf8B><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
-    case kGf8D: elementwise_kernel<kGf8D><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
-    case kGf16: elementwise_kernel<kGf16><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
-    case kGf32: elementwise_kernel<kGf32><<<blocks, 256, 0, s>>>(dst, a, b, nelem); break;
+    case kGf8B: elementwise_kernel<kGf8B><<<blocks, 256, 0, s>>>(dst, a, b, len, head, nvec); break;
+    case kGf8D: elementwise_kernel<kGf8D><<<blocks, 256, 0, s>>>(dst, a, b, len, head, nvec); break;
+    case kGf16: elementwise_kernel<kGf16><<<blocks, 256, 0, s>>>(dst, a, b, len, head, nvec); break;
+    case kGf32: elementwise_kernel<kGf32><<<blocks, 256, 0, s>>>(dst, a, b, len, head, nvec); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

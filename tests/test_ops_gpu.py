@@ -483,6 +483,28 @@ def test_elementwise_products_match_field_arithmetic(cuda, field):
         assert np.array_equal(h(got), want), ln
 
 
+@pytest.mark.parametrize("field", [Gf8B, Gf8D, Gf16, Gf32])
+@pytest.mark.parametrize("offsets", [(0, 0, 0), (4, 4, 4), (1, 1, 1), (2, 2, 2), (0, 3, 8)],
+                         ids=["aligned", "same4", "same1", "same2", "mixed"])
+def test_elementwise_alignments_and_long_rows(cuda, field, offsets):
+    """The kernel runs 16-byte vectors when dst, a and b share their offset
+    within 16 bytes and the bytes before the first boundary are whole
+    elements, and one element per step otherwise (and for heads and tails)."""
+    rng = np.random.default_rng(0xE1 + field.ID)
+    for ln in (field.BYTES, 7 * field.BYTES, 4096 + 3 * field.BYTES, (1 << 20) + 5 * field.BYTES):
+        a_h = rng.integers(0, 256, size=ln, dtype=np.uint8)
+        b_h = rng.integers(0, 256, size=ln, dtype=np.uint8)
+        a_h[:min(ln, 8)] = 0  # zero operands
+        pool = torch.zeros(3 * (ln + 64), dtype=torch.uint8, device="cuda")
+        views = [pool[i * (ln + 64) + o:i * (ln + 64) + o + ln] for i, o in enumerate(offsets)]
+        views[1].copy_(torch.from_numpy(a_h))
+        views[2].copy_(torch.from_numpy(b_h))
+        ops.mul_elementwise(field, views[0], views[1], views[2])
+        want = np.zeros(ln, np.uint8)
+        orc.mul_elementwise(field.ID, want, a_h, b_h)
+        assert np.array_equal(h(views[0]), want), (ln, offsets)
+
+
 def test_zero_and_one_coefficients_behave(cuda):
     # tests/ops.rs:881-895
     ln = 96
