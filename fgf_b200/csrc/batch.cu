@@ -375,6 +375,97 @@ __global__ void __launch_bounds__(kFastThreads, 1)
   }
 }
 
+// Segmented variant for byte-table classes whose sub-jobs have their own
+// plans (a batched reconstruct: one decode plan per erasure pattern). The
+// class's 16-byte columns are flattened in plan order (vprefix over the
+// class's sub-jobs jidx[]) and every CTA takes one contiguous range of equal
+// size, in whole rows of blockDim.x columns. A CTA sweeps its range like the
+// uniform kernel sweeps the whole class: the threads take consecutive
+// columns, so the CTA streams through one window of each source at a time,
+// and it loads pointers (and, if the plan differs, tables) only where its
+// range crosses into the next sub-job -- once or twice per CTA. Short work
+// items claimed from a counter (batch_fast_kernel) drain the memory pipeline
+// at every item boundary instead; that kernel keeps the scalar heads and
+// tails of the class.
+template <int K, bool SHIFT>
+__global__ void __launch_bounds__(kFastThreads, 1)
+    batch_fast_segment_kernel(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
+                              const uint32_t* __restrict__ jidx, const uint64_t* __restrict__ vprefix,
+                              uint32_t njobs) {
+  __shared__ const uint32_t* s_tab;
+  __shared__ uint32_t s_g0;
+  __shared__ const uint8_t* s_src[K];
+  __shared__ uint8_t* s_dst[4];
+  const uint64_t vtotal = vprefix[njobs];
+  const uint64_t rows = (vtotal + blockDim.x - 1) / blockDim.x;
+  const uint64_t chunk = (rows + gridDim.x - 1) / gridDim.x * blockDim.x;
+  uint64_t v0 = static_cast<uint64_t>(blockIdx.x) * chunk;
+  const uint64_t v1 = v0 + chunk < vtotal ? v0 + chunk : vtotal;
+  if (v0 >= v1) return;  // the whole CTA: no barrier is skipped by part of it
+  // the sub-job holding column v0: the last q with vprefix[q] <= v0
+  uint32_t lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (vprefix[mid] <= v0) lo = mid; else hi = mid;
+  }
+  uint32_t q = lo;
+  if (threadIdx.x == 0) {
+    s_tab = nullptr;
+    s_g0 = 0xFFFFFFFFu;
+  }
+  const FastRegs r;
+  const uint32_t lane = threadIdx.x & 31u;
+  while (v0 < v1) {
+    while (vprefix[q + 1] <= v0) ++q;  // sub-jobs without vectors
+    const uint64_t base = vprefix[q];
+    const uint64_t vend = vprefix[q + 1] < v1 ? vprefix[q + 1] : v1;
+    const BatchJob J = jobs[jidx[q]];
+    __syncthreads();  // the previous sub-job is done with tables and pointers
+    const bool resident = s_tab == J.tables && s_g0 == J.g0;
+    if (threadIdx.x < K) s_src[threadIdx.x] = reinterpret_cast<const uint8_t*>(ptrs[J.src_idx + threadIdx.x]);
+    if (threadIdx.x < J.nrows) s_dst[threadIdx.x] = reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + threadIdx.x]);
+    if (!resident) {
+      fill_fast<K>(J.tables, nullptr, J.gstride, J.g0);
+      if (threadIdx.x == 0) {
+        s_tab = J.tables;
+        s_g0 = J.g0;
+      }
+    }
+    __syncthreads();
+    const bool ovr = J.ovr != 0;
+    // SHIFT: whole warps iterate together (the row stores shuffle between
+    // lanes) and lanes past the end reload the last column
+    for (uint64_t ub = v0 + threadIdx.x - (SHIFT ? lane : 0u); ub < vend; ub += blockDim.x) {
+      const uint64_t u0 = SHIFT ? ub + lane : ub;
+      const bool valid = !SHIFT || u0 < vend;
+      const uint64_t u = valid ? u0 : vend - 1;
+      const uint64_t off = J.head + (u - base) * 16u;
+      if (u + blockDim.x < vend) {  // this thread's next column: into L2 now
+#pragma unroll
+        for (int t = 0; t < K; ++t) prefetch_l2(s_src[t] + off + blockDim.x * 16u);
+      }
+      uint32_t w[K][4];
+#pragma unroll
+      for (int t = 0; t < K; ++t) {
+        const uint4 x = ldg16(s_src[t] + off);
+        w[t][0] = x.x;
+        w[t][1] = x.y;
+        w[t][2] = x.z;
+        w[t][3] = x.w;
+      }
+      uint32_t acc[16];
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc[e] = 0;
+      fast_fold<K, 4>(w, acc, r);
+      if constexpr (SHIFT)
+        store_col4_any(acc, s_dst, J.nrows, off, ovr, valid);
+      else
+        store_col4(acc, s_dst, J.nrows, off, ovr);
+    }
+    v0 = vend;
+  }
+}
+
 // Uniform-plan variant: every sub-job of the class shares one plan, so each
 // CTA loads the tables once and grid-strides over the flattened column space
 // of all sub-jobs (vector columns first, then scalar groups), exactly like one
@@ -479,6 +570,7 @@ __global__ void __launch_bounds__(kFastThreads, 1)
 
 using KernelFn = void (*)(const BatchJob*, const uint64_t*, const uint2*, uint32_t, uint32_t*);
 using UniformFn = void (*)(UniformParams);
+using SegmentFn = void (*)(const BatchJob*, const uint64_t*, const uint32_t*, const uint64_t*, uint32_t);
 
 template <bool S>
 KernelFn kernel_for_s(int E, int G) {
@@ -507,6 +599,16 @@ KernelFn fast_kernel_for(int K, bool shift) {
   switch (K) {
 #define FGFC_CASE(k) \
   case k: return shift ? batch_fast_kernel<k, true> : batch_fast_kernel<k, false>;
+    FGFC_K_CASES(FGFC_CASE)
+#undef FGFC_CASE
+    default: return nullptr;
+  }
+}
+
+SegmentFn segment_kernel_for(int K, bool shift) {
+  switch (K) {
+#define FGFC_CASE(k) \
+  case k: return shift ? batch_fast_segment_kernel<k, true> : batch_fast_segment_kernel<k, false>;
     FGFC_K_CASES(FGFC_CASE)
 #undef FGFC_CASE
     default: return nullptr;
@@ -544,6 +646,8 @@ struct BatchClass {
   int K = 0;                   // > 0: byte-table class of Gf8 sub-jobs with K sources
   std::vector<uint32_t> jobs;  // sub-job indices, plan order
   std::vector<uint2> items;
+  std::vector<uint32_t> seg_jobs;   // byte-table class with own plans: sub-jobs with vectors, plan order
+  std::vector<uint64_t> seg_prefix; // and the prefix of their vector counts (the segmented launch)
   bool uniform = false;        // byte-table class whose sub-jobs share one plan
   bool shift = false;          // its rows are not all at the sources' offset within 16 bytes
 };
@@ -707,7 +811,19 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
       const uint64_t ngroups = (L.head + 3) / 4 + (tail + 3) / 4;
       const uint64_t ns_items = (ngroups + per_grp - 1) / per_grp;
       dj[i].nv_items = static_cast<uint32_t>(nv_items);
-      for (uint64_t p = 0; p < nv_items + ns_items; ++p) c.items.push_back(make_uint2(i, static_cast<unsigned>(p)));
+      if (c.K > 0) {
+        // vectors: the segmented launch; scalar heads and tails: work items
+        if (L.nvec) {
+          if (c.seg_prefix.empty()) c.seg_prefix.push_back(0);
+          c.seg_jobs.push_back(i);
+          c.seg_prefix.push_back(c.seg_prefix.back() + L.nvec);
+        }
+        for (uint64_t p = nv_items; p < nv_items + ns_items; ++p)
+          c.items.push_back(make_uint2(i, static_cast<unsigned>(p)));
+      } else {
+        for (uint64_t p = 0; p < nv_items + ns_items; ++p)
+          c.items.push_back(make_uint2(i, static_cast<unsigned>(p)));
+      }
     }
   }
 
@@ -718,15 +834,23 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
   const size_t off_ptrs = off;
   off = align16(off + ptrs.size() * sizeof(uint64_t));
   std::vector<std::pair<size_t, size_t>> cb;  // (items, counter) offsets
+  std::vector<std::pair<size_t, size_t>> sb;  // (segment jobs, segment prefix) offsets
   for (auto& kv : classes) {
-    std::pair<size_t, size_t> x{0, 0};
+    std::pair<size_t, size_t> x{0, 0}, y{0, 0};
     if (!kv.second.uniform) {
       x.first = off;
       off = align16(off + kv.second.items.size() * sizeof(uint2));
       x.second = off;
       off = align16(off + 64);
+      if (!kv.second.seg_jobs.empty()) {
+        y.first = off;
+        off = align16(off + kv.second.seg_jobs.size() * sizeof(uint32_t));
+        y.second = off;
+        off = align16(off + kv.second.seg_prefix.size() * sizeof(uint64_t));
+      }
     }
     cb.push_back(x);
+    sb.push_back(y);
   }
   // tensor-core bodies: one launch per plan (bit matrix), its stripes'
   // pointers and first blocks in the blob
@@ -774,10 +898,15 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
   {
     size_t ci = 0;
     for (auto& kv : classes) {
+      const auto& y = sb[ci];
       const auto& x = cb[ci++];
       if (kv.second.uniform) continue;
       std::memcpy(s.host + x.first, kv.second.items.data(), kv.second.items.size() * sizeof(uint2));
       std::memset(s.host + x.second, 0, 64);
+      if (!kv.second.seg_jobs.empty()) {
+        std::memcpy(s.host + y.first, kv.second.seg_jobs.data(), kv.second.seg_jobs.size() * sizeof(uint32_t));
+        std::memcpy(s.host + y.second, kv.second.seg_prefix.data(), kv.second.seg_prefix.size() * sizeof(uint64_t));
+      }
     }
     for (const TcGroup& G : tcg) {
       uint64_t* hp = reinterpret_cast<uint64_t*>(s.host + G.off_ptrs);
@@ -806,6 +935,9 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
     uint32_t* counter = nullptr;
     size_t uparam = 0;
     int tc_group = -1;  // >= 0: a tensor-core launch over that group's stripes
+    SegmentFn sfn = nullptr;  // segmented launch over the class's vectors
+    const uint32_t* seg_jobs = nullptr;
+    const uint64_t* seg_prefix = nullptr;
   };
   std::vector<Launch> launches;
   std::vector<UniformParams>& uparams = b->uparams;
@@ -815,6 +947,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
   size_t ci = 0;
   for (auto& kv : classes) {
     const BatchClass& c = kv.second;
+    const auto& y = sb[ci];
     const auto& x = cb[ci++];
     const bool fast = c.K > 0;
     Launch L;
@@ -869,13 +1002,31 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
       }
       b->last_items += c.jobs.size();
     } else {
-      L.n = static_cast<uint32_t>(c.items.size());
-      L.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((L.n + kClaim - 1) / kClaim, sms)));
-      L.items = reinterpret_cast<const uint2*>(s.dev + x.first);
-      L.counter = reinterpret_cast<uint32_t*>(s.dev + x.second);
-      b->last_items += c.items.size();
-      key += "|" + std::to_string(akey) + "," + std::to_string(L.n) + "," + std::to_string(L.grid);
-      launches.push_back(L);
+      if (!c.seg_jobs.empty()) {
+        Launch S = L;
+        S.fn = nullptr;
+        S.sfn = segment_kernel_for(c.K, c.shift);
+        if (!S.sfn) return cudaErrorInvalidValue;
+        e = ensure_smem_attr(reinterpret_cast<const void*>(S.sfn), static_cast<int>(S.smem));
+        if (e != cudaSuccess) return e;
+        S.n = static_cast<uint32_t>(c.seg_jobs.size());
+        S.seg_jobs = reinterpret_cast<const uint32_t*>(s.dev + y.first);
+        S.seg_prefix = reinterpret_cast<const uint64_t*>(s.dev + y.second);
+        const uint64_t rows = (c.seg_prefix.back() + S.threads - 1) / S.threads;
+        S.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(rows, sms)));
+        b->last_items += c.seg_jobs.size();
+        key += "|s" + std::to_string(akey) + "," + std::to_string(S.n) + "," + std::to_string(S.grid);
+        launches.push_back(S);
+      }
+      if (!c.items.empty()) {
+        L.n = static_cast<uint32_t>(c.items.size());
+        L.grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((L.n + kClaim - 1) / kClaim, sms)));
+        L.items = reinterpret_cast<const uint2*>(s.dev + x.first);
+        L.counter = reinterpret_cast<uint32_t*>(s.dev + x.second);
+        b->last_items += c.items.size();
+        key += "|" + std::to_string(akey) + "," + std::to_string(L.n) + "," + std::to_string(L.grid);
+        launches.push_back(L);
+      }
     }
   }
   for (size_t g = 0; g < tcg.size(); ++g) {
@@ -926,6 +1077,9 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
                                   static_cast<uint32_t>(G.idx.size()), G.nblk, J0.ovr, ls);
       } else if (L.ufn) {
         L.ufn<<<L.grid, L.threads, L.smem, ls>>>(uparams[L.uparam]);
+        err = cudaGetLastError();
+      } else if (L.sfn) {
+        L.sfn<<<L.grid, L.threads, L.smem, ls>>>(djobs, dptrs, L.seg_jobs, L.seg_prefix, L.n);
         err = cudaGetLastError();
       } else {
         L.fn<<<L.grid, L.threads, L.smem, ls>>>(djobs, dptrs, L.items, L.n, L.counter);
