@@ -949,7 +949,7 @@ def run_ours(args):
             "reconstruct": {"ms": round(rec_ms, 4), "GB/s": round(rec_bytes / rec_ms / 1e6, 1),
                             "frac": round(rec_bytes / rec_ms / 1e6 / peak, 4),
                             "source_GB/s": round(nst * K_SRC * L / rec_ms / 1e6, 1),
-                            "kernel": "batch_fast_kernel<10> (work-list, per-stripe decode plans, overwrite)"},
+                            "kernel": "batch_fast_segment_kernel<10> (contiguous column range per CTA, per-stripe decode plans, overwrite)"},
             "note": "achieved = algorithmic bytes of both submissions / their CUDA-event time; the rebuild "
                     "overwrites the erased rows, so it reads 10 and writes 4 shards per stripe"}
 
