@@ -42,7 +42,7 @@ fgfc_status cuda_fail(cudaError_t e, const char* what) {
   return fail(FGFC_ERR_CUDA, "%s: CUDA error: %s", what, cudaGetErrorString(e));
 }
 
-bool valid_field(int f) { return f >= 0 && f <= 3; }
+bool valid_field(int f) { return f >= 0 && f <= 6; }
 
 size_t zu(size_t v) { return v; }
 

@@ -641,21 +641,19 @@ void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t
   std::memset(bits, 0, kMaxOutBits * (kMaxInBits / 32) * sizeof(uint32_t));
   for (size_t t = 0; t < k; ++t)
     for (size_t j = 0; j < m; ++j) {
-      uint8_t M[4][4];
-      coeff_byte_matrix(field, coeffs[t * m + j] & field_mask(field), M);
-      for (int o = 0; o < E; ++o)
-        for (int p = 0; p < E; ++p) {
-          if (!M[o][p]) continue;
-          const size_t u = t * E + p;
-          for (int b = 0; b < 8; ++b) {
-            const uint8_t prod = byte_mul(field, M[o][p], static_cast<uint8_t>(1u << b));
-            for (int ob = 0; ob < 8; ++ob)
-              if ((prod >> ob) & 1u) {
-                const size_t n = (j * E + o) * 8 + ob;
-                bits[n * (kMaxInBits / 32) + u / 4] |= 1u << (8 * (u % 4) + b);
-              }
-          }
+      uint32_t img[4][8];
+      coeff_images(field, coeffs[t * m + j], img);
+      for (int p = 0; p < E; ++p) {
+        const size_t u = t * E + p;
+        for (int b = 0; b < 8; ++b) {
+          const uint32_t prod = img[p][b];  // c * (bit b of input byte p), E bytes
+          for (int ob = 0; ob < 8 * E; ++ob)
+            if ((prod >> ob) & 1u) {
+              const size_t n = j * E * 8 + ob;
+              bits[n * (kMaxInBits / 32) + u / 4] |= 1u << (8 * (u % 4) + b);
+            }
         }
+      }
     }
 }
 

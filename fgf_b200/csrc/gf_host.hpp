@@ -6,6 +6,9 @@
 //   Gf8D: GF(2)[x]/(x^8+x^4+x^3+x^2+1), generator 0x02   (src/field/gf8d.rs:40)
 //   Gf16: Gf8B[u]/(u^2+u+0x20), element a + b*u stored [a, b]  (src/field/gf16.rs:54-60)
 //   Gf32: Gf16[v]/(v^2+v+0x2000), element a + b*v stored LE    (src/field/gf32.rs:36-42)
+//   Fp8/Fp16/Fp32: the canonical Fan-Paar tower: the 2h-bit level is
+//         h-bit[X]/(X^2 + alpha X + 1), alpha the h-bit level's top generator,
+//         element lo + hi*X stored LE                            (src/field/fan_paar.rs:1-150)
 // inv(0) = 0 and x/0 = 0 by convention (src/field/mod.rs:38-41).
 #pragma once
 #include <cstddef>
@@ -13,19 +16,36 @@
 
 namespace fgfc {
 
-enum Field : int { kGf8B = 0, kGf8D = 1, kGf16 = 2, kGf32 = 3 };
+enum Field : int { kGf8B = 0, kGf8D = 1, kGf16 = 2, kGf32 = 3, kFp8 = 4, kFp16 = 5, kFp32 = 6 };
 
-inline int field_bytes(int f) { return f == kGf16 ? 2 : (f == kGf32 ? 4 : ((f == kGf8B || f == kGf8D) ? 1 : 0)); }
+inline int field_bytes(int f) {
+  switch (f) {
+    case kGf8B:
+    case kGf8D:
+    case kFp8: return 1;
+    case kGf16:
+    case kFp16: return 2;
+    case kGf32:
+    case kFp32: return 4;
+    default: return 0;
+  }
+}
 inline const char* field_name(int f) {
   switch (f) {
     case kGf8B: return "GF(2^8)";
     case kGf8D: return "GF(2^8)/0x11D";
     case kGf16: return "GF(2^16)";
     case kGf32: return "GF(2^32)";
+    case kFp8: return "Fan-Paar GF(2^8)";
+    case kFp16: return "Fan-Paar GF(2^16)";
+    case kFp32: return "Fan-Paar GF(2^32)";
     default: return "?";
   }
 }
-inline uint32_t field_mask(int f) { return f == kGf32 ? 0xFFFFFFFFu : (f == kGf16 ? 0xFFFFu : 0xFFu); }
+inline uint32_t field_mask(int f) {
+  const int E = field_bytes(f);
+  return E == 4 ? 0xFFFFFFFFu : (E == 2 ? 0xFFFFu : 0xFFu);
+}
 
 // Log/antilog tables for one flat GF(2^8), built from the generator by
 // repeated carry-less doubling with reduction.
@@ -89,12 +109,51 @@ inline uint32_t gf32_inv(uint32_t x) {
   return static_cast<uint32_t>(gf16_mul(a ^ b, ni)) | (static_cast<uint32_t>(gf16_mul(b, ni)) << 16);
 }
 
+// Fan-Paar tower arithmetic over `bits`-bit values (bits a power of two).
+// Products recurse by Karatsuba, z = (z0 + z2) + (z1 + alpha z2) X with
+// z0 = a0 b0, z2 = a1 b1, z1 = (a0 + a1)(b0 + b1) + z0 + z2; multiplying by
+// alpha (the level's top generator) is the linear recurrence
+// alpha (a0 + a1 X) = a1 + (a0 + alpha' a1) X one level down; the inverse is
+// the conjugate (a0 + alpha a1) - a1 X over the norm a0 (a0 + alpha a1) + a1^2.
+inline uint32_t fp_low(unsigned bits) { return bits >= 32 ? 0xFFFFFFFFu : ((1u << bits) - 1u); }
+
+inline uint32_t fp_mul_alpha(uint32_t v, unsigned bits) {
+  if (bits == 1) return v & 1u;
+  const unsigned h = bits / 2;
+  const uint32_t a0 = v & fp_low(h), a1 = v >> h;
+  return a1 | ((a0 ^ fp_mul_alpha(a1, h)) << h);
+}
+
+inline uint32_t fp_mul(uint32_t x, uint32_t y, unsigned bits) {
+  if (bits == 1) return x & y & 1u;
+  const unsigned h = bits / 2;
+  const uint32_t m = fp_low(h);
+  const uint32_t a0 = x & m, a1 = x >> h, b0 = y & m, b1 = y >> h;
+  const uint32_t z0 = fp_mul(a0, b0, h), z2 = fp_mul(a1, b1, h);
+  const uint32_t z1 = fp_mul(a0 ^ a1, b0 ^ b1, h) ^ z0 ^ z2;
+  return (z0 ^ z2) | ((z1 ^ fp_mul_alpha(z2, h)) << h);
+}
+
+inline uint32_t fp_inv(uint32_t x, unsigned bits) {
+  if (bits == 1) return x & 1u;
+  const unsigned h = bits / 2;
+  const uint32_t a0 = x & fp_low(h), a1 = x >> h;
+  const uint32_t conj0 = a0 ^ fp_mul_alpha(a1, h);
+  const uint32_t ni = fp_inv(fp_mul(a0, conj0, h) ^ fp_mul(a1, a1, h), h);
+  return fp_mul(ni, conj0, h) | (fp_mul(ni, a1, h) << h);
+}
+
+inline unsigned fp_bits(int f) { return 8u * static_cast<unsigned>(field_bytes(f)); }
+
 inline uint32_t gf_mul(int f, uint32_t a, uint32_t b) {
   switch (f) {
     case kGf8B: return gf8b_tab().mul(a & 0xFF, b & 0xFF);
     case kGf8D: return gf8d_tab().mul(a & 0xFF, b & 0xFF);
     case kGf16: return gf16_mul(a & 0xFFFF, b & 0xFFFF);
     case kGf32: return gf32_mul(a, b);
+    case kFp8:
+    case kFp16:
+    case kFp32: return fp_mul(a & field_mask(f), b & field_mask(f), fp_bits(f));
     default: return 0;
   }
 }
@@ -105,51 +164,32 @@ inline uint32_t gf_inv(int f, uint32_t a) {
     case kGf8D: return gf8d_tab().inv(a & 0xFF);
     case kGf16: return gf16_inv(a & 0xFFFF);
     case kGf32: return gf32_inv(a);
+    case kFp8:
+    case kFp16:
+    case kFp32: return fp_inv(a & field_mask(f), fp_bits(f));
     default: return 0;
   }
 }
 
-// Multiplying a packed element by a fixed coefficient is linear over the
-// byte subfield: output byte o = XOR_p M[o][p] * input byte p, products in
-// the byte field (Gf8D for Gf8D, Gf8B otherwise). Fills M[0..E)[0..E).
-//   Gf8 : M = [c]
-//   Gf16: (a + b u)(c0 + c1 u) = (c0 a + 0x20 c1 b) + (c1 a + (c0 + c1) b) u
-//   Gf32: the same identity one level up, each Gf16 product a 2x2 block.
-inline void coeff_byte_matrix(int f, uint32_t c, uint8_t M[4][4]) {
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 4; ++j) M[i][j] = 0;
-  if (f == kGf8B || f == kGf8D) {
-    M[0][0] = c & 0xFF;
-    return;
-  }
-  auto m16 = [](uint16_t x, uint8_t out[2][2]) {
-    const uint8_t x0 = x & 0xFF, x1 = x >> 8;
-    out[0][0] = x0;
-    out[0][1] = gf8b_mul(0x20, x1);
-    out[1][0] = x1;
-    out[1][1] = x0 ^ x1;
-  };
-  if (f == kGf16) {
-    uint8_t b[2][2];
-    m16(static_cast<uint16_t>(c), b);
-    for (int i = 0; i < 2; ++i)
-      for (int j = 0; j < 2; ++j) M[i][j] = b[i][j];
-    return;
-  }
-  const uint16_t c0 = c & 0xFFFF, c1 = c >> 16;
-  const uint16_t blocks[2][2] = {{c0, gf16_mul(0x2000, c1)}, {c1, static_cast<uint16_t>(c0 ^ c1)}};
-  for (int bi = 0; bi < 2; ++bi)
-    for (int bj = 0; bj < 2; ++bj) {
-      uint8_t b[2][2];
-      m16(blocks[bi][bj], b);
-      for (int i = 0; i < 2; ++i)
-        for (int j = 0; j < 2; ++j) M[2 * bi + i][2 * bj + j] = b[i][j];
-    }
+// Multiplying a packed element by a fixed coefficient c is linear over
+// GF(2) in every field here. img[p][b] is c times the element whose only set
+// bit is bit b of byte p (an E-byte value), so that for an input element x,
+// byte o of c * x = XOR over the set bits (p, b) of x of byte o of img[p][b].
+// Every table the kernels use (nibble and byte tables, GF(2) bit matrices)
+// is derived from these images, for any field.
+inline void coeff_images(int f, uint32_t c, uint32_t img[4][8]) {
+  const int E = field_bytes(f);
+  for (int p = 0; p < 4; ++p)
+    for (int b = 0; b < 8; ++b)
+      img[p][b] = p < E ? gf_mul(f, c & field_mask(f), 1u << (8 * p + b)) : 0u;
 }
 
-// Byte-subfield product used by the tables of field f.
-inline uint8_t byte_mul(int f, uint8_t a, uint8_t b) {
-  return f == kGf8D ? gf8d_tab().mul(a, b) : gf8b_tab().mul(a, b);
+// Byte o of c * (x placed in input byte p), from the images.
+inline uint8_t image_byte(const uint32_t img[4][8], int p, uint8_t x, int o) {
+  uint32_t v = 0;
+  for (int b = 0; b < 8; ++b)
+    if ((x >> b) & 1u) v ^= img[p][b];
+  return static_cast<uint8_t>(v >> (8 * o));
 }
 
 }  // namespace fgfc

@@ -6,12 +6,12 @@
 // overwrite (dot_product*) or accumulate (mul_add*) semantics.
 //
 // Arithmetic: multiplying a packed element by a fixed coefficient is linear
-// over its byte subfield, so every output byte is an XOR of products of
-// source bytes with constants (gf_host.hpp: coeff_byte_matrix). Products are
+// over GF(2) in every field here, so every output byte is an XOR of fixed
+// linear maps of the source bytes (gf_host.hpp: coeff_images). Products are
 // read from split-nibble tables in shared memory: per (source, source byte
 // plane, group of 4 output bytes) a 16-entry table for the low nibble and
 // one for the high nibble, each entry a 32-bit word carrying the products
-// for 4 output bytes at once (4 Gf8 rows, 2 Gf16 rows or 1 Gf32 row). Every
+// for 4 output bytes at once (4 one-byte, 2 two-byte or 1 four-byte rows). Every
 // table row is replicated across the 32 banks so a warp's lookups never
 // conflict, and one PRMT forms each lookup address from the nibble, the
 // lane and the table slot. The destination tile stays in registers while all
@@ -489,6 +489,60 @@ __global__ void elementwise_kernel(uint8_t* __restrict__ dst, const uint8_t* __r
   }
 }
 
+// ---- mul_elementwise over the Fan-Paar towers. Byte products use the
+// byte level's log/exp tables (generator 0x2d) and a byte times the byte
+// level's top generator alpha uses a 256-entry table; the 16- and 32-bit
+// levels follow the Karatsuba recursion of the tower X^2 + alpha X + 1
+// (src/field/fan_paar.rs:80-94, 122-134). Tables: 1 KiB, staged from
+// constant memory into shared memory per CTA.
+__constant__ uint8_t c_fp_tab[1024];  // exp[0..510) | pad | log[256] | alpha[256]
+
+struct FpTab {
+  const uint8_t* exp;
+  const uint8_t* log;
+  const uint8_t* alpha;
+  __device__ __forceinline__ uint32_t m8(uint32_t a, uint32_t b) const {
+    return (a && b) ? exp[log[a] + log[b]] : 0u;
+  }
+  __device__ __forceinline__ uint32_t alpha16(uint32_t v) const {  // v * alpha at the 16-bit level
+    return (v >> 8) | (((v & 0xFFu) ^ alpha[v >> 8]) << 8);
+  }
+  __device__ __forceinline__ uint32_t m16(uint32_t x, uint32_t y) const {
+    const uint32_t a0 = x & 0xFFu, a1 = x >> 8, b0 = y & 0xFFu, b1 = y >> 8;
+    const uint32_t z0 = m8(a0, b0), z2 = m8(a1, b1), z1 = m8(a0 ^ a1, b0 ^ b1) ^ z0 ^ z2;
+    return (z0 ^ z2) | ((z1 ^ alpha[z2]) << 8);
+  }
+  __device__ __forceinline__ uint32_t m32(uint32_t x, uint32_t y) const {
+    const uint32_t a0 = x & 0xFFFFu, a1 = x >> 16, b0 = y & 0xFFFFu, b1 = y >> 16;
+    const uint32_t z0 = m16(a0, b0), z2 = m16(a1, b1), z1 = m16(a0 ^ a1, b0 ^ b1) ^ z0 ^ z2;
+    return (z0 ^ z2) | ((z1 ^ alpha16(z2)) << 16);
+  }
+};
+
+template <int E>
+__global__ void elementwise_fp_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ a,
+                                      const uint8_t* __restrict__ b, uint64_t nelem) {
+  __shared__ uint8_t tab[1024];
+  for (int i = threadIdx.x; i < 1024; i += blockDim.x) tab[i] = c_fp_tab[i];
+  __syncthreads();
+  const FpTab T{tab, tab + 512, tab + 768};
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem; i += stride) {
+    uint32_t x = 0, y = 0;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      x |= static_cast<uint32_t>(a[E * i + k]) << (8 * k);
+      y |= static_cast<uint32_t>(b[E * i + k]) << (8 * k);
+    }
+    const uint32_t r = E == 1 ? T.m8(x, y) : (E == 2 ? T.m16(x, y) : T.m32(x, y));
+#pragma unroll
+    for (int k = 0; k < E; ++k) dst[E * i + k] = static_cast<uint8_t>(r >> (8 * k));
+  }
+}
+
+std::atomic<bool> g_fp_ready[kMaxDevices];
+std::mutex g_fp_mu;
+
 }  // namespace
 
 int sm_count() {
@@ -557,11 +611,47 @@ cudaError_t launch_xor(uint8_t* dst, const uint8_t* src, uint64_t len, cudaStrea
   return cudaGetLastError();
 }
 
+// Fan-Paar fields: byte tables built on the host from the tower product,
+// uploaded once per device.
+static cudaError_t launch_elementwise_fp(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
+                                         uint64_t len, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_fp_ready[dev].load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> lk(g_fp_mu);
+    uint8_t tab[1024] = {};
+    uint32_t v = 1;
+    for (int i = 0; i < 255; ++i) {
+      tab[i] = tab[i + 255] = static_cast<uint8_t>(v);
+      tab[512 + v] = static_cast<uint8_t>(i);
+      v = fp_mul(v, 0x2D, 8);
+    }
+    for (uint32_t x = 0; x < 256; ++x) tab[768 + x] = static_cast<uint8_t>(fp_mul_alpha(x, 8));
+    e = cudaMemcpyToSymbol(c_fp_tab, tab, sizeof tab);
+    if (e != cudaSuccess) return e;
+    g_fp_ready[dev].store(true, std::memory_order_release);
+  }
+  const int E = field_bytes(field);
+  const uint64_t nelem = len / E;
+  uint64_t want = (nelem + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
+  const unsigned blocks = static_cast<unsigned>(want < cap ? want : cap);
+  if (E == 1)
+    elementwise_fp_kernel<1><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
+  else if (E == 2)
+    elementwise_fp_kernel<2><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
+  else
+    elementwise_fp_kernel<4><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const uint8_t* b,
                                uint64_t len, cudaStream_t s) {
   if (!len) return cudaSuccess;
   const int E = field_bytes(field);
   if (E <= 0 || len % E) return cudaErrorInvalidValue;
+  if (field == kFp8 || field == kFp16 || field == kFp32) return launch_elementwise_fp(field, dst, a, b, len, s);
   const uint64_t ad = reinterpret_cast<uintptr_t>(dst) & 15;
   uint64_t head = len, nvec = 0;
   if (ad == (reinterpret_cast<uintptr_t>(a) & 15) && ad == (reinterpret_cast<uintptr_t>(b) & 15)) {

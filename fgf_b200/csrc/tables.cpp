@@ -21,15 +21,15 @@ void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0
   for (size_t tt = 0; tt < k; ++tt) {
     const size_t t = t0 + tt;
     for (size_t g = 0; g < G; ++g) {
-      // Byte matrices of the R rows this group covers (rows past m
+      // Images of the R coefficients this group covers (rows past m
       // contribute zero products).
-      uint8_t M[4][4][4];
+      uint32_t img[4][4][8];
       for (int r = 0; r < R; ++r) {
         const size_t j = (g0 + g) * R + r;
         if (j < m) {
-          coeff_byte_matrix(field, coeffs[t * m + j], M[r]);
+          coeff_images(field, coeffs[t * m + j], img[r]);
         } else {
-          std::memset(M[r], 0, sizeof M[r]);
+          std::memset(img[r], 0, sizeof img[r]);
         }
       }
       for (int p = 0; p < E; ++p) {
@@ -39,7 +39,7 @@ void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0
             const uint8_t x = static_cast<uint8_t>(half ? (n << 4) : n);
             uint32_t word = 0;
             for (int q = 0; q < 4; ++q)
-              word |= static_cast<uint32_t>(byte_mul(field, M[q / E][q % E][p], x)) << (8 * q);
+              word |= static_cast<uint32_t>(image_byte(img[q / E], p, x, q % E)) << (8 * q);
             slot[half * 16 + n] = word;
           }
       }

@@ -1,4 +1,4 @@
-"""Field markers and host scalar arithmetic for the four fields of the hot path.
+"""Field markers and host scalar arithmetic for the fields of the hot path.
 
 Mirrors the reference's `Field` types (src/field/mod.rs:110-144): each marker
 carries `ID` (the fgfc_field code), `NAME`, `BYTES` and scalar `mul`, `inv`,
@@ -9,6 +9,7 @@ decode matrices (RS recipes below); vector work goes to the device.
   Gf8D: GF(2)[x]/(x^8+x^4+x^3+x^2+1), generator 0x02     (src/field/gf8d.rs:40)
   Gf16: Gf8B[u]/(u^2+u+0x20), bytes [a, b] for a + b*u   (src/field/gf16.rs:54-60)
   Gf32: Gf16[v]/(v^2+v+0x2000), little-endian halves     (src/field/gf32.rs:36-42)
+  FanPaar8/16/32: the canonical Fan-Paar tower           (src/field/fan_paar.rs)
 inv(0) = 0 and x/0 = 0 (src/field/mod.rs:38-41).
 """
 from __future__ import annotations
@@ -122,7 +123,84 @@ class Gf32:
         return m(a ^ b, ni) | (m(b, ni) << 16)
 
 
-FIELDS = {f.ID: f for f in (Gf8B, Gf8D, Gf16, Gf32)}
+def _fp_low(bits: int) -> int:
+    return (1 << bits) - 1
+
+
+def _fp_mul_alpha(v: int, bits: int) -> int:
+    """Multiply by a level's top tower generator (src/field/fan_paar.rs:67-76)."""
+    if bits == 1:
+        return v & 1
+    h = bits // 2
+    a0, a1 = v & _fp_low(h), v >> h
+    return a1 | ((a0 ^ _fp_mul_alpha(a1, h)) << h)
+
+
+def _fp_mul(x: int, y: int, bits: int) -> int:
+    """Karatsuba product of the tower X^2 + alpha X + 1 (fan_paar.rs:80-94)."""
+    if bits == 1:
+        return x & y & 1
+    h = bits // 2
+    m = _fp_low(h)
+    a0, a1, b0, b1 = x & m, x >> h, y & m, y >> h
+    z0, z2 = _fp_mul(a0, b0, h), _fp_mul(a1, b1, h)
+    z1 = _fp_mul(a0 ^ a1, b0 ^ b1, h) ^ z0 ^ z2
+    return (z0 ^ z2) | ((z1 ^ _fp_mul_alpha(z2, h)) << h)
+
+
+def _fp_inv(x: int, bits: int) -> int:
+    """Conjugate times inverse norm, inv(0) = 0 (fan_paar.rs:137-148)."""
+    if bits == 1:
+        return x & 1
+    h = bits // 2
+    a0, a1 = x & _fp_low(h), x >> h
+    a0z1 = a0 ^ _fp_mul_alpha(a1, h)
+    norm = _fp_mul(a0, a0z1, h) ^ _fp_mul(a1, a1, h)
+    ni = _fp_inv(norm, h)
+    return _fp_mul(ni, a0z1, h) | (_fp_mul(ni, a1, h) << h)
+
+
+class _FanPaar:
+    """Canonical Fan-Paar binary tower (src/field/fan_paar.rs:1-14): each
+    level of 2h bits is h-bit[X]/(X^2 + alpha X + 1), alpha the h-bit level's
+    own top generator; an element is lo + hi*X, lo in the low h bits."""
+    ID = -1
+    NAME = ""
+    BYTES = 1
+    BITS = 8
+    GENERATOR = 0
+
+    @classmethod
+    def mul(cls, a: int, b: int) -> int:
+        return _fp_mul(a & _fp_low(cls.BITS), b & _fp_low(cls.BITS), cls.BITS)
+
+    @classmethod
+    def inv(cls, a: int) -> int:
+        return _fp_inv(a & _fp_low(cls.BITS), cls.BITS)
+
+
+class FanPaar8(_FanPaar):
+    ID = 4
+    NAME = "Fan-Paar GF(2^8)"
+    BYTES, BITS = 1, 8
+    GENERATOR = 0x2D  # src/field/fan_paar.rs:537-548
+
+
+class FanPaar16(_FanPaar):
+    ID = 5
+    NAME = "Fan-Paar GF(2^16)"
+    BYTES, BITS = 2, 16
+    GENERATOR = 0xE2DE  # fan_paar.rs:549-562
+
+
+class FanPaar32(_FanPaar):
+    ID = 6
+    NAME = "Fan-Paar GF(2^32)"
+    BYTES, BITS = 4, 32
+    GENERATOR = 0x03E2_1CEA  # fan_paar.rs:563-576
+
+
+FIELDS = {f.ID: f for f in (Gf8B, Gf8D, Gf16, Gf32, FanPaar8, FanPaar16, FanPaar32)}
 
 
 def div(field, a: int, b: int) -> int:

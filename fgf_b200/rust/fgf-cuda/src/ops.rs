@@ -9,6 +9,7 @@
 use std::marker::PhantomData;
 use std::ptr;
 
+use fgf::fan_paar::{fp16, fp32, fp8, FanPaar16, FanPaar32, FanPaar8};
 use fgf::field::{gf16, gf32, gf8b, gf8d, Field, Gf16, Gf32, Gf8B, Gf8D};
 
 use crate::device::{DeviceSlice, DeviceSliceMut, Stream};
@@ -58,6 +59,36 @@ impl CudaField for Gf32 {
     }
     fn from_raw(v: u32) -> gf32::Elem {
         gf32::Elem(v)
+    }
+}
+
+impl CudaField for FanPaar8 {
+    const ID: sys::fgfc_field = sys::FGFC_FP8;
+    fn to_raw(e: fp8::Elem) -> u32 {
+        u32::from(e.0)
+    }
+    fn from_raw(v: u32) -> fp8::Elem {
+        fp8::Elem(v as u8)
+    }
+}
+
+impl CudaField for FanPaar16 {
+    const ID: sys::fgfc_field = sys::FGFC_FP16;
+    fn to_raw(e: fp16::Elem) -> u32 {
+        u32::from(e.0)
+    }
+    fn from_raw(v: u32) -> fp16::Elem {
+        fp16::Elem(v as u16)
+    }
+}
+
+impl CudaField for FanPaar32 {
+    const ID: sys::fgfc_field = sys::FGFC_FP32;
+    fn to_raw(e: fp32::Elem) -> u32 {
+        e.0
+    }
+    fn from_raw(v: u32) -> fp32::Elem {
+        fp32::Elem(v)
     }
 }
 

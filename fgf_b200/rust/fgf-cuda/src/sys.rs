@@ -13,6 +13,9 @@ pub const FGFC_GF8B: fgfc_field = 0;
 pub const FGFC_GF8D: fgfc_field = 1;
 pub const FGFC_GF16: fgfc_field = 2;
 pub const FGFC_GF32: fgfc_field = 3;
+pub const FGFC_FP8: fgfc_field = 4;
+pub const FGFC_FP16: fgfc_field = 5;
+pub const FGFC_FP32: fgfc_field = 6;
 
 pub const FGFC_OK: fgfc_status = 0;
 pub const FGFC_ERR_WIDTH: fgfc_status = 1;

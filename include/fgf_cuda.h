@@ -44,7 +44,13 @@ typedef enum fgfc_field {
   FGFC_GF8B = 0, /* GF(2^8) mod 0x11B, 1 byte */
   FGFC_GF8D = 1, /* GF(2^8) mod 0x11D, 1 byte */
   FGFC_GF16 = 2, /* (GF(2^8)/0x11B)[u]/(u^2+u+0x20), 2 bytes LE */
-  FGFC_GF32 = 3  /* GF(2^16)[v]/(v^2+v+0x2000), 4 bytes LE */
+  FGFC_GF32 = 3, /* GF(2^16)[v]/(v^2+v+0x2000), 4 bytes LE */
+  /* The canonical Fan-Paar binary tower (src/field/fan_paar.rs:1-150): the
+     2h-bit level is h-bit[X]/(X^2 + alpha X + 1), alpha the h-bit level's
+     top generator; elements lo + hi*X, little-endian. */
+  FGFC_FP8 = 4,  /* Fan-Paar GF(2^8), 1 byte  (fan_paar::fp8, FanPaar8) */
+  FGFC_FP16 = 5, /* Fan-Paar GF(2^16), 2 bytes (fan_paar::fp16, FanPaar16) */
+  FGFC_FP32 = 6  /* Fan-Paar GF(2^32), 4 bytes (fan_paar::fp32, FanPaar32) */
 } fgfc_field;
 
 typedef enum fgfc_status {

@@ -10,6 +10,8 @@
  *   - GF(2^16) tower a+b*u, u^2+u+0x20 over Gf8B, Karatsuba product and
  *     conjugate/norm inverse (src/field/gf16.rs:54-60,143-180);
  *   - GF(2^32) tower over GF(2^16), DELTA 0x2000 (src/field/gf32.rs:36-42,121-150);
+ *   - the canonical Fan-Paar towers at 8, 16 and 32 bits
+ *     (src/field/fan_paar.rs:1-14,66-150);
  *   - elementwise op semantics including the zero/one shortcuts
  *     (src/kernel/scalar.rs:20-130, src/ops.rs:342-941).
  */
@@ -98,6 +100,49 @@ static uint32_t gf32_inv(uint32_t x) {
   return (uint32_t)gf16_mul((uint16_t)(a ^ b), ni) | ((uint32_t)gf16_mul(b, ni) << 16);
 }
 
+/* ---------------------------------------------------------------- Fan-Paar towers */
+/*
+ * Canonical Fan-Paar binary tower (src/field/fan_paar.rs:1-14,66-150): each
+ * level of 2h bits is the quadratic extension X^2 + alpha*X + 1 of the h-bit
+ * level, alpha being that level's own top generator; an element is
+ * lo + hi*X with lo in the low h bits. Products recurse by Karatsuba down to
+ * one bit (fan_paar.rs:80-94); multiplying by alpha is the linear recurrence
+ * of fan_paar.rs:67-76; inversion is conjugate times inverse norm
+ * (fan_paar.rs:137-148).
+ */
+static uint32_t fp_low(unsigned bits) { return bits >= 32 ? 0xFFFFFFFFu : ((1u << bits) - 1u); }
+
+static uint32_t fp_mul_alpha(uint32_t v, unsigned bits) {
+  if (bits == 1) return v & 1u;
+  unsigned h = bits / 2;
+  uint32_t a0 = v & fp_low(h), a1 = v >> h;
+  return a1 | ((a0 ^ fp_mul_alpha(a1, h)) << h);
+}
+
+static uint32_t fp_mul_bits(uint32_t x, uint32_t y, unsigned bits) {
+  if (bits == 1) return x & y & 1u;
+  unsigned h = bits / 2;
+  uint32_t m = fp_low(h);
+  uint32_t a0 = x & m, a1 = x >> h, b0 = y & m, b1 = y >> h;
+  uint32_t z0 = fp_mul_bits(a0, b0, h), z2 = fp_mul_bits(a1, b1, h);
+  uint32_t z1 = fp_mul_bits(a0 ^ a1, b0 ^ b1, h) ^ z0 ^ z2;
+  return (z0 ^ z2) | ((z1 ^ fp_mul_alpha(z2, h)) << h);
+}
+
+static uint32_t fp_square_bits(uint32_t x, unsigned bits) { return fp_mul_bits(x, x, bits); }
+
+static uint32_t fp_inv_bits(uint32_t x, unsigned bits) {
+  if (bits == 1) return x & 1u;
+  unsigned h = bits / 2;
+  uint32_t a0 = x & fp_low(h), a1 = x >> h;
+  uint32_t a0z1 = a0 ^ fp_mul_alpha(a1, h);
+  uint32_t norm = fp_mul_bits(a0, a0z1, h) ^ fp_square_bits(a1, h);
+  uint32_t ni = fp_inv_bits(norm, h);
+  return fp_mul_bits(ni, a0z1, h) | (fp_mul_bits(ni, a1, h) << h);
+}
+
+static unsigned fp_bits(int field) { return field == ORC_FP8 ? 8u : (field == ORC_FP16 ? 16u : 32u); }
+
 /* ---------------------------------------------------------------- public scalar API */
 
 int orc_bytes(int field) {
@@ -106,6 +151,9 @@ int orc_bytes(int field) {
     case ORC_GF8D: return 1;
     case ORC_GF16: return 2;
     case ORC_GF32: return 4;
+    case ORC_FP8: return 1;
+    case ORC_FP16: return 2;
+    case ORC_FP32: return 4;
     default: return 0;
   }
 }
@@ -116,6 +164,12 @@ uint32_t orc_mul(int field, uint32_t a, uint32_t b) {
     case ORC_GF8D: return gf8_mul(1, (uint8_t)a, (uint8_t)b);
     case ORC_GF16: return gf16_mul((uint16_t)a, (uint16_t)b);
     case ORC_GF32: return gf32_mul(a, b);
+    case ORC_FP8:
+    case ORC_FP16:
+    case ORC_FP32: {
+      unsigned bits = fp_bits(field);
+      return fp_mul_bits(a & fp_low(bits), b & fp_low(bits), bits);
+    }
     default: return 0;
   }
 }
@@ -132,6 +186,12 @@ uint32_t orc_inv(int field, uint32_t a) {
     case ORC_GF8D: return gf8_inv(1, (uint8_t)a);
     case ORC_GF16: return gf16_inv((uint16_t)a);
     case ORC_GF32: return gf32_inv(a);
+    case ORC_FP8:
+    case ORC_FP16:
+    case ORC_FP32: {
+      unsigned bits = fp_bits(field);
+      return fp_inv_bits(a & fp_low(bits), bits);
+    }
     default: return 0;
   }
 }

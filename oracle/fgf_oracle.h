@@ -12,7 +12,8 @@
  * src/kernel/tables.rs tests); see tests/test_oracle_pins.py.
  *
  * Field ids: 0 = Gf8B (0x11B), 1 = Gf8D (0x11D), 2 = Gf16 (tower over Gf8B),
- * 3 = Gf32 (tower over Gf16). Elements are passed as uint32_t values; buffers
+ * 3 = Gf32 (tower over Gf16), 4 / 5 / 6 = canonical Fan-Paar GF(2^8) /
+ * GF(2^16) / GF(2^32). Elements are passed as uint32_t values; buffers
  * hold packed little-endian elements exactly as the reference's `ops` does.
  *
  * Coefficient matrices for the many-to-many ops are passed term-major:
@@ -29,7 +30,7 @@
 extern "C" {
 #endif
 
-enum { ORC_GF8B = 0, ORC_GF8D = 1, ORC_GF16 = 2, ORC_GF32 = 3 };
+enum { ORC_GF8B = 0, ORC_GF8D = 1, ORC_GF16 = 2, ORC_GF32 = 3, ORC_FP8 = 4, ORC_FP16 = 5, ORC_FP32 = 6 };
 
 int orc_bytes(int field);
 

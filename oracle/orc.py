@@ -14,6 +14,7 @@ import numpy as np
 from . import build as _build
 
 GF8B, GF8D, GF16, GF32 = 0, 1, 2, 3
+FP8, FP16, FP32 = 4, 5, 6  # canonical Fan-Paar towers (src/field/fan_paar.rs)
 
 _L: C.CDLL | None = None
 

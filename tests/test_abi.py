@@ -50,3 +50,19 @@ def test_rust_crate_binds_every_entry_point():
                "mul_add_gather_with", "dot_product", "dot_product_with", "mul_add_matrix", "mul_add_matrix_with",
                "dot_product_matrix", "dot_product_matrix_with", "mul_add_matrix_scattered"):
         assert op in wrapped, f"ops.rs lacks {op}"
+
+
+def test_field_codes_agree_across_header_python_and_rust():
+    """fgfc_field codes: the header enum, the Python field markers and the
+    crate's constants and CudaField impls name the same fields."""
+    from fgf_b200.fields import FIELDS
+
+    text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "fgf_cuda.h").read_text(), flags=re.S)
+    enum = {name: int(v) for name, v in re.findall(r"\b(FGFC_(?:GF|FP)[0-9A-Z]+)\s*=\s*(\d+)", text)}
+    sys_rs = (ROOT / "fgf_b200" / "rust" / "fgf-cuda" / "src" / "sys.rs").read_text()
+    rust = {name: int(v) for name, v in re.findall(r"pub const (FGFC_(?:GF|FP)[0-9A-Z]+): fgfc_field = (\d+);", sys_rs)}
+    assert enum == rust
+    assert sorted(enum.values()) == sorted(FIELDS)
+    ops_rs = (ROOT / "fgf_b200" / "rust" / "fgf-cuda" / "src" / "ops.rs").read_text()
+    impls = set(re.findall(r"const ID: sys::fgfc_field = sys::(FGFC_[0-9A-Z]+);", ops_rs))
+    assert impls == set(enum)
