@@ -9,7 +9,8 @@ decode matrices (RS recipes below); vector work goes to the device.
   Gf8D: GF(2)[x]/(x^8+x^4+x^3+x^2+1), generator 0x02     (src/field/gf8d.rs:40)
   Gf16: Gf8B[u]/(u^2+u+0x20), bytes [a, b] for a + b*u   (src/field/gf16.rs:54-60)
   Gf32: Gf16[v]/(v^2+v+0x2000), little-endian halves     (src/field/gf32.rs:36-42)
-  FanPaar8/16/32: the canonical Fan-Paar tower           (src/field/fan_paar.rs)
+  Gf64: Gf32[w]/(w^2+w+0x20000000), little-endian halves (src/field/gf64.rs:1-11)
+  FanPaar8/16/32/64: the canonical Fan-Paar tower        (src/field/fan_paar.rs)
 inv(0) = 0 and x/0 = 0 (src/field/mod.rs:38-41).
 """
 from __future__ import annotations
@@ -200,7 +201,42 @@ class FanPaar32(_FanPaar):
     GENERATOR = 0x03E2_1CEA  # fan_paar.rs:563-576
 
 
-FIELDS = {f.ID: f for f in (Gf8B, Gf8D, Gf16, Gf32, FanPaar8, FanPaar16, FanPaar32)}
+class FanPaar64(_FanPaar):
+    ID = 8
+    NAME = "Fan-Paar GF(2^64)"
+    BYTES, BITS = 8, 64
+    GENERATOR = 0x070F_870D_CD9C_1D88  # fan_paar.rs:577-590
+
+
+class Gf64:
+    """GF(2^64) = Gf32[w]/(w^2 + w + 0x20000000), a + b*w with a in the low
+    half (src/field/gf64.rs:1-11,120-151)."""
+    ID = 7
+    NAME = "GF(2^64)"
+    BYTES = 8
+    BITS = 64
+    DELTA = 0x2000_0000
+    GENERATOR = 0x0000_0001_0000_0004
+
+    @staticmethod
+    def mul(x: int, y: int) -> int:
+        a, b, c, d = x & 0xFFFFFFFF, x >> 32, y & 0xFFFFFFFF, y >> 32
+        m = Gf32.mul
+        ac, bd = m(a, c), m(b, d)
+        return (ac ^ m(0x2000_0000, bd)) | ((m(a ^ b, c ^ d) ^ ac) << 32)
+
+    @staticmethod
+    def inv(x: int) -> int:
+        if x == 0:
+            return 0
+        a, b = x & 0xFFFFFFFF, x >> 32
+        m = Gf32.mul
+        norm = m(a, a) ^ m(a, b) ^ m(0x2000_0000, m(b, b))
+        ni = Gf32.inv(norm)
+        return m(a ^ b, ni) | (m(b, ni) << 32)
+
+
+FIELDS = {f.ID: f for f in (Gf8B, Gf8D, Gf16, Gf32, FanPaar8, FanPaar16, FanPaar32, Gf64, FanPaar64)}
 
 
 def div(field, a: int, b: int) -> int:

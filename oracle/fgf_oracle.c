@@ -10,7 +10,8 @@
  *   - GF(2^16) tower a+b*u, u^2+u+0x20 over Gf8B, Karatsuba product and
  *     conjugate/norm inverse (src/field/gf16.rs:54-60,143-180);
  *   - GF(2^32) tower over GF(2^16), DELTA 0x2000 (src/field/gf32.rs:36-42,121-150);
- *   - the canonical Fan-Paar towers at 8, 16 and 32 bits
+ *   - GF(2^64) tower over GF(2^32), DELTA 0x20000000 (src/field/gf64.rs:1-11,120-151);
+ *   - the canonical Fan-Paar towers at 8, 16, 32 and 64 bits
  *     (src/field/fan_paar.rs:1-14,66-150);
  *   - elementwise op semantics including the zero/one shortcuts
  *     (src/kernel/scalar.rs:20-130, src/ops.rs:342-941).
@@ -110,38 +111,57 @@ static uint32_t gf32_inv(uint32_t x) {
  * of fan_paar.rs:67-76; inversion is conjugate times inverse norm
  * (fan_paar.rs:137-148).
  */
-static uint32_t fp_low(unsigned bits) { return bits >= 32 ? 0xFFFFFFFFu : ((1u << bits) - 1u); }
+static uint64_t fp_low(unsigned bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1ull); }
 
-static uint32_t fp_mul_alpha(uint32_t v, unsigned bits) {
+static uint64_t fp_mul_alpha(uint64_t v, unsigned bits) {
   if (bits == 1) return v & 1u;
   unsigned h = bits / 2;
-  uint32_t a0 = v & fp_low(h), a1 = v >> h;
+  uint64_t a0 = v & fp_low(h), a1 = v >> h;
   return a1 | ((a0 ^ fp_mul_alpha(a1, h)) << h);
 }
 
-static uint32_t fp_mul_bits(uint32_t x, uint32_t y, unsigned bits) {
+static uint64_t fp_mul_bits(uint64_t x, uint64_t y, unsigned bits) {
   if (bits == 1) return x & y & 1u;
   unsigned h = bits / 2;
-  uint32_t m = fp_low(h);
-  uint32_t a0 = x & m, a1 = x >> h, b0 = y & m, b1 = y >> h;
-  uint32_t z0 = fp_mul_bits(a0, b0, h), z2 = fp_mul_bits(a1, b1, h);
-  uint32_t z1 = fp_mul_bits(a0 ^ a1, b0 ^ b1, h) ^ z0 ^ z2;
+  uint64_t m = fp_low(h);
+  uint64_t a0 = x & m, a1 = x >> h, b0 = y & m, b1 = y >> h;
+  uint64_t z0 = fp_mul_bits(a0, b0, h), z2 = fp_mul_bits(a1, b1, h);
+  uint64_t z1 = fp_mul_bits(a0 ^ a1, b0 ^ b1, h) ^ z0 ^ z2;
   return (z0 ^ z2) | ((z1 ^ fp_mul_alpha(z2, h)) << h);
 }
 
-static uint32_t fp_square_bits(uint32_t x, unsigned bits) { return fp_mul_bits(x, x, bits); }
-
-static uint32_t fp_inv_bits(uint32_t x, unsigned bits) {
+static uint64_t fp_inv_bits(uint64_t x, unsigned bits) {
   if (bits == 1) return x & 1u;
   unsigned h = bits / 2;
-  uint32_t a0 = x & fp_low(h), a1 = x >> h;
-  uint32_t a0z1 = a0 ^ fp_mul_alpha(a1, h);
-  uint32_t norm = fp_mul_bits(a0, a0z1, h) ^ fp_square_bits(a1, h);
-  uint32_t ni = fp_inv_bits(norm, h);
+  uint64_t a0 = x & fp_low(h), a1 = x >> h;
+  uint64_t a0z1 = a0 ^ fp_mul_alpha(a1, h);
+  uint64_t norm = fp_mul_bits(a0, a0z1, h) ^ fp_mul_bits(a1, a1, h);
+  uint64_t ni = fp_inv_bits(norm, h);
   return fp_mul_bits(ni, a0z1, h) | (fp_mul_bits(ni, a1, h) << h);
 }
 
-static unsigned fp_bits(int field) { return field == ORC_FP8 ? 8u : (field == ORC_FP16 ? 16u : 32u); }
+static unsigned fp_bits(int field) {
+  return field == ORC_FP8 ? 8u : (field == ORC_FP16 ? 16u : (field == ORC_FP32 ? 32u : 64u));
+}
+
+/* GF(2^64) = GF(2^32)[w]/(w^2 + w + 0x20000000), a + b*w with a in the low
+ * half (src/field/gf64.rs:1-11,120-151): the same Karatsuba product and
+ * conjugate / norm inverse as one level down. */
+static uint64_t gf64_mul(uint64_t x, uint64_t y) {
+  uint32_t a = (uint32_t)x, b = (uint32_t)(x >> 32), c = (uint32_t)y, d = (uint32_t)(y >> 32);
+  uint32_t ac = gf32_mul(a, c), bd = gf32_mul(b, d);
+  uint32_t lo = ac ^ gf32_mul(0x20000000u, bd);
+  uint32_t hi = gf32_mul(a ^ b, c ^ d) ^ ac;
+  return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+
+static uint64_t gf64_inv(uint64_t x) {
+  uint32_t a = (uint32_t)x, b = (uint32_t)(x >> 32);
+  if (x == 0) return 0;
+  uint32_t norm = gf32_mul(a, a) ^ gf32_mul(a, b) ^ gf32_mul(0x20000000u, gf32_mul(b, b));
+  uint32_t ni = gf32_inv(norm);
+  return (uint64_t)gf32_mul(a ^ b, ni) | ((uint64_t)gf32_mul(b, ni) << 32);
+}
 
 /* ---------------------------------------------------------------- public scalar API */
 
@@ -154,6 +174,8 @@ int orc_bytes(int field) {
     case ORC_FP8: return 1;
     case ORC_FP16: return 2;
     case ORC_FP32: return 4;
+    case ORC_GF64:
+    case ORC_FP64: return 8;
     default: return 0;
   }
 }
@@ -168,7 +190,7 @@ uint32_t orc_mul(int field, uint32_t a, uint32_t b) {
     case ORC_FP16:
     case ORC_FP32: {
       unsigned bits = fp_bits(field);
-      return fp_mul_bits(a & fp_low(bits), b & fp_low(bits), bits);
+      return (uint32_t)fp_mul_bits(a & fp_low(bits), b & fp_low(bits), bits);
     }
     default: return 0;
   }
@@ -190,7 +212,7 @@ uint32_t orc_inv(int field, uint32_t a) {
     case ORC_FP16:
     case ORC_FP32: {
       unsigned bits = fp_bits(field);
-      return fp_inv_bits(a & fp_low(bits), bits);
+      return (uint32_t)fp_inv_bits(a & fp_low(bits), bits);
     }
     default: return 0;
   }
@@ -225,6 +247,28 @@ uint32_t orc_pow(int field, uint32_t a, uint64_t e) {
   return r;
 }
 
+uint64_t orc_mul64(int field, uint64_t a, uint64_t b) {
+  if (field == ORC_GF64) return gf64_mul(a, b);
+  if (field == ORC_FP64) return fp_mul_bits(a, b, 64);
+  return orc_mul(field, (uint32_t)a, (uint32_t)b);
+}
+
+uint64_t orc_inv64(int field, uint64_t a) {
+  if (field == ORC_GF64) return gf64_inv(a);
+  if (field == ORC_FP64) return fp_inv_bits(a, 64);
+  return orc_inv(field, (uint32_t)a);
+}
+
+uint64_t orc_pow64(int field, uint64_t a, uint64_t e) {
+  uint64_t base = a, r = 1;
+  while (e) {
+    if (e & 1) r = orc_mul64(field, r, base);
+    base = orc_mul64(field, base, base);
+    e >>= 1;
+  }
+  return r;
+}
+
 void orc_noise(uint8_t *out, size_t len, uint64_t seed) {
   uint64_t s = seed | 1u;
   for (size_t i = 0; i < len; ++i) {
@@ -235,15 +279,14 @@ void orc_noise(uint8_t *out, size_t len, uint64_t seed) {
 
 /* ---------------------------------------------------------------- element I/O */
 
-static uint32_t rd(int field, const uint8_t *p) {
-  switch (orc_bytes(field)) {
-    case 1: return p[0];
-    case 2: return (uint32_t)p[0] | ((uint32_t)p[1] << 8);
-    default: return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
-  }
+static uint64_t rd(int field, const uint8_t *p) {
+  int n = orc_bytes(field);
+  uint64_t v = 0;
+  for (int i = 0; i < n; ++i) v |= (uint64_t)p[i] << (8 * i);
+  return v;
 }
 
-static void wr(int field, uint8_t *p, uint32_t v) {
+static void wr(int field, uint8_t *p, uint64_t v) {
   int n = orc_bytes(field);
   for (int i = 0; i < n; ++i) p[i] = (uint8_t)(v >> (8 * i));
 }
@@ -254,50 +297,50 @@ void orc_xor(uint8_t *dst, const uint8_t *src, size_t len) {
   for (size_t i = 0; i < len; ++i) dst[i] ^= src[i];
 }
 
-void orc_mul_add(int field, uint8_t *dst, uint32_t coeff, const uint8_t *src, size_t len) {
+void orc_mul_add(int field, uint8_t *dst, uint64_t coeff, const uint8_t *src, size_t len) {
   /* scalar.rs:40-57: zero is a no-op, one is XOR, otherwise per element. */
   if (coeff == 0) return;
   if (coeff == 1) { orc_xor(dst, src, len); return; }
   int b = orc_bytes(field);
   for (size_t i = 0; i + b <= len; i += b)
-    wr(field, dst + i, rd(field, dst + i) ^ orc_mul(field, rd(field, src + i), coeff));
+    wr(field, dst + i, rd(field, dst + i) ^ orc_mul64(field, rd(field, src + i), coeff));
 }
 
-void orc_mul_into(int field, uint8_t *dst, uint32_t coeff, const uint8_t *src, size_t len) {
+void orc_mul_into(int field, uint8_t *dst, uint64_t coeff, const uint8_t *src, size_t len) {
   /* ops.rs:381-392 */
   if (coeff == 0) { memset(dst, 0, len); return; }
   if (coeff == 1) { memmove(dst, src, len); return; }
   int b = orc_bytes(field);
-  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul(field, rd(field, src + i), coeff));
+  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul64(field, rd(field, src + i), coeff));
 }
 
-void orc_mul_assign(int field, uint8_t *dst, uint32_t coeff, size_t len) {
+void orc_mul_assign(int field, uint8_t *dst, uint64_t coeff, size_t len) {
   /* scalar.rs:60-72 */
   if (coeff == 1) return;
   if (coeff == 0) { memset(dst, 0, len); return; }
   int b = orc_bytes(field);
-  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul(field, rd(field, dst + i), coeff));
+  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul64(field, rd(field, dst + i), coeff));
 }
 
 void orc_mul_elementwise(int field, uint8_t *dst, const uint8_t *a, const uint8_t *bb, size_t len) {
   /* scalar.rs:119-130 */
   int b = orc_bytes(field);
-  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul(field, rd(field, a + i), rd(field, bb + i)));
+  for (size_t i = 0; i + b <= len; i += b) wr(field, dst + i, orc_mul64(field, rd(field, a + i), rd(field, bb + i)));
 }
 
-void orc_mul_add_scatter(int field, uint8_t *rows, size_t row_len, const uint32_t *coeffs,
+void orc_mul_add_scatter(int field, uint8_t *rows, size_t row_len, const uint64_t *coeffs,
                          size_t nrows, const uint8_t *src) {
   /* scalar.rs:75-79: one mul_add per row. */
   for (size_t j = 0; j < nrows; ++j) orc_mul_add(field, rows + j * row_len, coeffs[j], src, row_len);
 }
 
-void orc_mul_add_gather(int field, uint8_t *dst, size_t len, const uint32_t *coeffs,
+void orc_mul_add_gather(int field, uint8_t *dst, size_t len, const uint64_t *coeffs,
                         const uint8_t *const *srcs, size_t nsrcs) {
   /* scalar.rs:112-116 */
   for (size_t t = 0; t < nsrcs; ++t) orc_mul_add(field, dst, coeffs[t], srcs[t], len);
 }
 
-void orc_dot_product(int field, uint8_t *dst, size_t len, const uint32_t *coeffs,
+void orc_dot_product(int field, uint8_t *dst, size_t len, const uint64_t *coeffs,
                      const uint8_t *const *srcs, size_t nsrcs) {
   /* ops.rs:597-624: overwrite; empty or all-zero fills zero. */
   memset(dst, 0, len);
@@ -305,7 +348,7 @@ void orc_dot_product(int field, uint8_t *dst, size_t len, const uint32_t *coeffs
 }
 
 void orc_mul_add_matrix(int field, uint8_t *rows, size_t row_len, size_t nrows,
-                        const uint32_t *coeffs, const uint8_t *const *srcs, size_t nsrcs) {
+                        const uint64_t *coeffs, const uint8_t *const *srcs, size_t nsrcs) {
   /* scalar.rs:82-94: every term applied to every row. */
   for (size_t t = 0; t < nsrcs; ++t)
     for (size_t j = 0; j < nrows; ++j)
@@ -313,7 +356,7 @@ void orc_mul_add_matrix(int field, uint8_t *rows, size_t row_len, size_t nrows,
 }
 
 void orc_dot_product_matrix(int field, uint8_t *rows, size_t row_len, size_t nrows,
-                            const uint32_t *coeffs, const uint8_t *const *srcs, size_t nsrcs) {
+                            const uint64_t *coeffs, const uint8_t *const *srcs, size_t nsrcs) {
   /* ops.rs:773-810 / kernel/mod.rs:507-533: zero the used rows, accumulate. */
   memset(rows, 0, row_len * nrows);
   orc_mul_add_matrix(field, rows, row_len, nrows, coeffs, srcs, nsrcs);
@@ -321,7 +364,7 @@ void orc_dot_product_matrix(int field, uint8_t *rows, size_t row_len, size_t nro
 
 void orc_mul_add_matrix_scattered(int field, uint8_t *dst, size_t row_len,
                                   const size_t *row_starts, size_t nrows,
-                                  const uint32_t *coeffs, const uint8_t *const *srcs,
+                                  const uint64_t *coeffs, const uint8_t *const *srcs,
                                   size_t nsrcs) {
   /* scalar.rs:98-109 */
   for (size_t t = 0; t < nsrcs; ++t)

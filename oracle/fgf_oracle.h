@@ -13,7 +13,9 @@
  *
  * Field ids: 0 = Gf8B (0x11B), 1 = Gf8D (0x11D), 2 = Gf16 (tower over Gf8B),
  * 3 = Gf32 (tower over Gf16), 4 / 5 / 6 = canonical Fan-Paar GF(2^8) /
- * GF(2^16) / GF(2^32). Elements are passed as uint32_t values; buffers
+ * GF(2^16) / GF(2^32), 7 = Gf64 (tower over Gf32), 8 = Fan-Paar GF(2^64).
+ * Scalars are uint32_t (uint64_t in the *64 functions), op coefficients
+ * uint64_t; buffers
  * hold packed little-endian elements exactly as the reference's `ops` does.
  *
  * Coefficient matrices for the many-to-many ops are passed term-major:
@@ -30,7 +32,8 @@
 extern "C" {
 #endif
 
-enum { ORC_GF8B = 0, ORC_GF8D = 1, ORC_GF16 = 2, ORC_GF32 = 3, ORC_FP8 = 4, ORC_FP16 = 5, ORC_FP32 = 6 };
+enum { ORC_GF8B = 0, ORC_GF8D = 1, ORC_GF16 = 2, ORC_GF32 = 3, ORC_FP8 = 4, ORC_FP16 = 5, ORC_FP32 = 6,
+       ORC_GF64 = 7, ORC_FP64 = 8 };
 
 int orc_bytes(int field);
 
@@ -42,29 +45,33 @@ uint32_t orc_inv_xtime(int field, uint32_t a);             /* Gf8 Fermat form */
 uint32_t orc_div(int field, uint32_t a, uint32_t b);       /* x / 0 == 0 */
 uint32_t orc_pow(int field, uint32_t a, uint64_t e);
 uint32_t orc_square(int field, uint32_t a);
+/* The same for every field, 8-byte ones included (values as uint64_t). */
+uint64_t orc_mul64(int field, uint64_t a, uint64_t b);
+uint64_t orc_inv64(int field, uint64_t a);
+uint64_t orc_pow64(int field, uint64_t a, uint64_t e);
 
 /* The reference tests' deterministic byte stream (tests/ops.rs:17-27). */
 void orc_noise(uint8_t *out, size_t len, uint64_t seed);
 
 /* Elementwise op semantics (src/kernel/scalar.rs, src/ops.rs). */
 void orc_xor(uint8_t *dst, const uint8_t *src, size_t len);
-void orc_mul_add(int field, uint8_t *dst, uint32_t coeff, const uint8_t *src, size_t len);
-void orc_mul_into(int field, uint8_t *dst, uint32_t coeff, const uint8_t *src, size_t len);
-void orc_mul_assign(int field, uint8_t *dst, uint32_t coeff, size_t len);
+void orc_mul_add(int field, uint8_t *dst, uint64_t coeff, const uint8_t *src, size_t len);
+void orc_mul_into(int field, uint8_t *dst, uint64_t coeff, const uint8_t *src, size_t len);
+void orc_mul_assign(int field, uint8_t *dst, uint64_t coeff, size_t len);
 void orc_mul_elementwise(int field, uint8_t *dst, const uint8_t *a, const uint8_t *b, size_t len);
-void orc_mul_add_scatter(int field, uint8_t *rows, size_t row_len, const uint32_t *coeffs,
+void orc_mul_add_scatter(int field, uint8_t *rows, size_t row_len, const uint64_t *coeffs,
                          size_t nrows, const uint8_t *src);
-void orc_mul_add_gather(int field, uint8_t *dst, size_t len, const uint32_t *coeffs,
+void orc_mul_add_gather(int field, uint8_t *dst, size_t len, const uint64_t *coeffs,
                         const uint8_t *const *srcs, size_t nsrcs);
-void orc_dot_product(int field, uint8_t *dst, size_t len, const uint32_t *coeffs,
+void orc_dot_product(int field, uint8_t *dst, size_t len, const uint64_t *coeffs,
                      const uint8_t *const *srcs, size_t nsrcs);
 void orc_mul_add_matrix(int field, uint8_t *rows, size_t row_len, size_t nrows,
-                        const uint32_t *coeffs, const uint8_t *const *srcs, size_t nsrcs);
+                        const uint64_t *coeffs, const uint8_t *const *srcs, size_t nsrcs);
 void orc_dot_product_matrix(int field, uint8_t *rows, size_t row_len, size_t nrows,
-                            const uint32_t *coeffs, const uint8_t *const *srcs, size_t nsrcs);
+                            const uint64_t *coeffs, const uint8_t *const *srcs, size_t nsrcs);
 void orc_mul_add_matrix_scattered(int field, uint8_t *dst, size_t row_len,
                                   const size_t *row_starts, size_t nrows,
-                                  const uint32_t *coeffs, const uint8_t *const *srcs,
+                                  const uint64_t *coeffs, const uint8_t *const *srcs,
                                   size_t nsrcs);
 
 /* Reed-Solomon recipes built on the field arithmetic (caller-side in the

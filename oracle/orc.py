@@ -15,6 +15,7 @@ from . import build as _build
 
 GF8B, GF8D, GF16, GF32 = 0, 1, 2, 3
 FP8, FP16, FP32 = 4, 5, 6  # canonical Fan-Paar towers (src/field/fan_paar.rs)
+GF64, FP64 = 7, 8  # GF(2^64) over GF(2^32) (src/field/gf64.rs), Fan-Paar GF(2^64)
 
 _L: C.CDLL | None = None
 
@@ -35,6 +36,13 @@ def L() -> C.CDLL:
             getattr(_L, name).argtypes = [C.c_int, u32]
         _L.orc_pow.restype = u32
         _L.orc_pow.argtypes = [C.c_int, u32, C.c_uint64]
+        u64 = C.c_uint64
+        _L.orc_mul64.restype = u64
+        _L.orc_mul64.argtypes = [C.c_int, u64, u64]
+        _L.orc_inv64.restype = u64
+        _L.orc_inv64.argtypes = [C.c_int, u64]
+        _L.orc_pow64.restype = u64
+        _L.orc_pow64.argtypes = [C.c_int, u64, u64]
         _L.orc_noise.argtypes = [p, sz, C.c_uint64]
         _L.orc_invert.restype = C.c_int
         _L.orc_decode_matrix.restype = C.c_int
@@ -47,6 +55,10 @@ def _p(a: np.ndarray) -> C.c_void_p:
 
 def _u32(v) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(v, dtype=np.uint64).astype(np.uint32))
+
+
+def _u64(v) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray([int(x) for x in np.asarray(v).reshape(-1)], dtype=np.uint64))
 
 
 def _ptrs(srcs) -> C.Array:
@@ -77,6 +89,19 @@ def pow_(f, a, e):
     return L().orc_pow(f, a, e)
 
 
+def mul64(f, a, b):
+    """Product in any field, 8-byte ones included."""
+    return L().orc_mul64(f, a, b)
+
+
+def inv64(f, a):
+    return L().orc_inv64(f, a)
+
+
+def pow64(f, a, e):
+    return L().orc_pow64(f, a, e)
+
+
 def noise(n: int, seed: int) -> np.ndarray:
     """The reference tests' LCG byte stream (tests/ops.rs:17-27)."""
     out = np.empty(n, dtype=np.uint8)
@@ -86,15 +111,15 @@ def noise(n: int, seed: int) -> np.ndarray:
 
 
 def mul_add(f, dst: np.ndarray, c: int, src: np.ndarray) -> None:
-    L().orc_mul_add(f, _p(dst), C.c_uint32(c), _p(src), C.c_size_t(len(dst)))
+    L().orc_mul_add(f, _p(dst), C.c_uint64(c), _p(src), C.c_size_t(len(dst)))
 
 
 def mul_into(f, dst, c, src) -> None:
-    L().orc_mul_into(f, _p(dst), C.c_uint32(c), _p(src), C.c_size_t(len(dst)))
+    L().orc_mul_into(f, _p(dst), C.c_uint64(c), _p(src), C.c_size_t(len(dst)))
 
 
 def mul_assign(f, dst, c) -> None:
-    L().orc_mul_assign(f, _p(dst), C.c_uint32(c), C.c_size_t(len(dst)))
+    L().orc_mul_assign(f, _p(dst), C.c_uint64(c), C.c_size_t(len(dst)))
 
 
 def mul_elementwise(f, dst, a, b) -> None:
@@ -102,34 +127,34 @@ def mul_elementwise(f, dst, a, b) -> None:
 
 
 def mul_add_scatter(f, rows, row_len, coeffs, src) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     L().orc_mul_add_scatter(f, _p(rows), C.c_size_t(row_len), _p(c), C.c_size_t(len(c)), _p(src))
 
 
 def mul_add_gather(f, dst, coeffs, srcs) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     L().orc_mul_add_gather(f, _p(dst), C.c_size_t(len(dst)), _p(c), _ptrs(srcs), C.c_size_t(len(srcs)))
 
 
 def dot_product(f, dst, coeffs, srcs) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     L().orc_dot_product(f, _p(dst), C.c_size_t(len(dst)), _p(c), _ptrs(srcs), C.c_size_t(len(srcs)))
 
 
 def mul_add_matrix(f, rows, row_len, nrows, coeffs, srcs) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     L().orc_mul_add_matrix(f, _p(rows), C.c_size_t(row_len), C.c_size_t(nrows), _p(c), _ptrs(srcs),
                            C.c_size_t(len(srcs)))
 
 
 def dot_product_matrix(f, rows, row_len, nrows, coeffs, srcs) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     L().orc_dot_product_matrix(f, _p(rows), C.c_size_t(row_len), C.c_size_t(nrows), _p(c), _ptrs(srcs),
                                C.c_size_t(len(srcs)))
 
 
 def mul_add_matrix_scattered(f, dst, row_len, row_starts, coeffs, srcs) -> None:
-    c = _u32(coeffs)
+    c = _u64(coeffs)
     st = (C.c_size_t * max(1, len(row_starts)))(*row_starts)
     L().orc_mul_add_matrix_scattered(f, _p(dst), C.c_size_t(row_len), st, C.c_size_t(len(row_starts)),
                                      _p(c), _ptrs(srcs), C.c_size_t(len(srcs)))

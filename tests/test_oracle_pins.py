@@ -242,3 +242,54 @@ def test_fan_paar_byte_products_nest():
 def test_fan_paar_names():
     for name, (_, host) in FPF.items():
         assert host.NAME == FP["names"][name]
+
+
+# ---------------------------------------------------------------- 8-byte fields
+WIDE = GOLD["wide_fields"]
+
+
+def test_gf64_schoolbook_inverse_and_order():
+    # tests/algebra.rs:412-420,439-471
+    vals = [int(v, 16) for v in WIDE["gf64_sample"]["values"]]
+    delta = int(WIDE["gf64_sample"]["delta"], 16)
+
+    def school(x, y):
+        a, b, c, d = x & 0xFFFFFFFF, x >> 32, y & 0xFFFFFFFF, y >> 32
+        m = lambda u, v: orc.mul(orc.GF32, u, v)  # noqa: E731
+        return (m(a, c) ^ m(delta, m(b, d))) | ((m(a, d) ^ m(b, c) ^ m(b, d)) << 32)
+
+    for i, a in enumerate(vals):
+        b = vals[(i * 7 + 3) % len(vals)]
+        assert orc.mul64(orc.GF64, a, b) == school(a, b) == fields.Gf64.mul(a, b)
+        if a:
+            assert orc.mul64(orc.GF64, a, orc.inv64(orc.GF64, a)) == 1
+            assert fields.Gf64.mul(a, fields.Gf64.inv(a)) == 1
+    g = int(WIDE["gf64_generator"]["generator"], 16)
+    assert fields.Gf64.GENERATOR == g
+    assert orc.pow64(orc.GF64, g, (1 << 64) - 1) == 1
+    for q in WIDE["gf64_generator"]["factors"]:
+        assert orc.pow64(orc.GF64, g, ((1 << 64) - 1) // q) != 1
+
+
+def test_fan_paar_64_vectors():
+    # tests/algebra.rs:491-494,517-523,547-551,555-576
+    for case in WIDE["fp64_products"]:
+        a, b, want = (int(case[k], 16) for k in ("a", "b", "product"))
+        assert orc.mul64(orc.FP64, a, b) == want == fields.FanPaar64.mul(a, b)
+    for v in WIDE["fp64_round_trip_values"]["values"]:
+        a = int(v, 16)
+        if a:
+            assert orc.mul64(orc.FP64, a, orc.inv64(orc.FP64, a)) == 1
+            assert fields.FanPaar64.mul(a, fields.FanPaar64.inv(a)) == 1
+    g = int(WIDE["fp64_generator"]["generator"], 16)
+    assert fields.FanPaar64.GENERATOR == g
+    assert orc.pow64(orc.FP64, g, (1 << 64) - 1) == 1
+    for q in WIDE["fp64_generator"]["factors"]:
+        assert orc.pow64(orc.FP64, g, ((1 << 64) - 1) // q) != 1
+    for a, b in FP["nested_byte_products"]["pairs"]:
+        a, b = int(a, 16), int(b, 16)
+        assert orc.mul64(orc.FP64, a, b) == orc.mul(orc.FP8, a, b)
+
+
+def test_wide_field_names():
+    assert fields.Gf64.NAME == WIDE["names"]["gf64"] and fields.FanPaar64.NAME == WIDE["names"]["fp64"]
