@@ -148,6 +148,10 @@ _SIGS = {
     "fgfc_plan_len": (c_size, [C.c_void_p]),
     "fgfc_plan_field": (C.c_int, [C.c_void_p]),
     "fgfc_plan_values": (c_status, [C.c_void_p, C.POINTER(c_u32)]),
+    "fgfc_plan_create_u64": (c_status, [C.c_int, c_size, c_size, C.POINTER(C.c_uint64), C.POINTER(C.c_void_p)]),
+    "fgfc_coeff_create_u64": (c_status, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "fgfc_plan_values_u64": (c_status, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "fgfc_plan_get_at_u64": (c_status, [C.c_void_p, c_size, c_size, C.POINTER(C.c_uint64)]),
     "fgfc_plan_get_at": (c_status, [C.c_void_p, c_size, c_size, C.POINTER(c_u32)]),
     "fgfc_add_assign": (c_status, [C.c_int, c_u8p, c_size, c_u8p, c_size, c_stream]),
     "fgfc_mul_add": (c_status, [C.c_int, c_u8p, c_size, c_u32, c_u8p, c_size, c_stream]),

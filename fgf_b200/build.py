@@ -22,7 +22,7 @@ LIB = PKG / "libfgfcuda.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["kernels.cu", "batch.cu", "gf2mma.cu", "api.cpp", "tables.cpp", "serve.cpp", "decode.cpp",
+SOURCES = ["kernels.cu", "batch.cu", "gf2mma.cu", "wide.cu", "api.cpp", "tables.cpp", "serve.cpp", "decode.cpp",
            "tune.cpp"]
 FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
 

@@ -42,7 +42,7 @@ fgfc_status cuda_fail(cudaError_t e, const char* what) {
   return fail(FGFC_ERR_CUDA, "%s: CUDA error: %s", what, cudaGetErrorString(e));
 }
 
-bool valid_field(int f) { return f >= 0 && f <= 6; }
+bool valid_field(int f) { return f >= 0 && f <= 8; }
 
 size_t zu(size_t v) { return v; }
 
@@ -79,7 +79,7 @@ bool mul_overflows(size_t a, size_t b, size_t* out) {
 struct fgfc_plan {
   int field;
   size_t rows, cols;
-  std::vector<uint32_t> values;
+  std::vector<uint64_t> values;  // coefficients, any field width
   // GF(2) bit matrices for the tensor-core kernel, per orientation (matrix:
   // rows x cols; scatter: 1 x len; gather: len x 1), empty where the shape
   // is outside that kernel's range
@@ -89,7 +89,7 @@ struct fgfc_plan {
   uint32_t* dev;        // device tables, three orientations back to back
   size_t mat_groups;    // groups per source in the matrix orientation
   size_t off_mat, off_scat, off_gath;  // word offsets into `dev`
-  size_t scat_groups;
+  size_t scat_groups, gath_groups;
 };
 
 namespace {
@@ -97,7 +97,7 @@ namespace {
 // Coefficient source for a lowered matrix call: either raw host values
 // (term-major, k x m) or device tables of a plan.
 struct CoeffSrc {
-  const uint32_t* host = nullptr;  // term-major k x m
+  const uint64_t* host = nullptr;  // term-major k x m
   const uint32_t* dev = nullptr;   // compact tables [(t*E+p)*gstride + g][32]
   size_t gstride = 0;
   const uint32_t* bits = nullptr;  // GF(2) bit matrix (plans), or built from `host` when needed
@@ -174,6 +174,10 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
     return ok();
   }
   const int E = field_bytes(field);
+  if (E == 8) {
+    cudaError_t e = wide_launch(field, srcs, k, rows, m, cs.host, cs.dev, cs.gstride, len, overwrite, stream);
+    return e == cudaSuccess ? ok() : cuda_fail(e, name);
+  }
   const int R = 4 / E;
   const size_t gtot = (m + R - 1) / R;
   const bool inl = cs.dev == nullptr;
@@ -237,7 +241,7 @@ fgfc_status run_matrix(int field, const uint8_t* const* srcs, size_t k, uint8_t*
   return ok();
 }
 
-bool all_zero(const uint32_t* c, size_t n, uint32_t mask) {
+bool all_zero(const uint64_t* c, size_t n, uint64_t mask) {
   for (size_t i = 0; i < n; ++i)
     if (c[i] & mask) return false;
   return true;
@@ -245,14 +249,16 @@ bool all_zero(const uint32_t* c, size_t n, uint32_t mask) {
 
 fgfc_status upload_plan_tables(fgfc_plan* p) {
   const int E = field_bytes(p->field);
-  const int R = 4 / E;
   const size_t len = p->values.size();
+  // 4-byte output groups covering n rows of E-byte elements
+  const auto groups = [E](size_t n) { return (n * E + 3) / 4; };
   // matrix orientation: rows = sources, cols = destination rows
-  p->mat_groups = p->cols ? (p->cols + R - 1) / R : 0;
+  p->mat_groups = groups(p->cols);
   const size_t n_mat = p->rows * E * p->mat_groups * kCompactWords;
-  p->scat_groups = len ? (len + R - 1) / R : 0;
+  p->scat_groups = groups(len);
   const size_t n_scat = E * p->scat_groups * kCompactWords;
-  const size_t n_gath = len * E * kCompactWords;
+  p->gath_groups = groups(1);
+  const size_t n_gath = len * E * p->gath_groups * kCompactWords;
   std::vector<uint32_t> host(n_mat + n_scat + n_gath + 1, 0);
   p->off_mat = 0;
   p->off_scat = n_mat;
@@ -263,7 +269,7 @@ fgfc_status upload_plan_tables(fgfc_plan* p) {
                                    host.data() + p->off_scat);
   if (n_gath) {
     // gather orientation: source i has the single coefficient values[i]
-    build_compact_tables(p->field, p->values.data(), 1, 0, len, 0, 1, host.data() + p->off_gath);
+    build_compact_tables(p->field, p->values.data(), 1, 0, len, 0, p->gath_groups, host.data() + p->off_gath);
   }
   if (n_mat && gf2mma_shape_ok(p->field, p->rows, p->cols)) {
     p->bits_mat.resize(kGf2BitWords);
@@ -307,12 +313,35 @@ CoeffSrc plan_scat(const fgfc_plan* p) {
 CoeffSrc plan_gath(const fgfc_plan* p) {
   CoeffSrc c;
   c.dev = p->dev + p->off_gath;
-  c.gstride = 1;
+  c.gstride = p->gath_groups;
   c.bits = p->bits_gath.empty() ? nullptr : p->bits_gath.data();
   return c;
 }
 
 }  // namespace
+
+template <typename C>
+static fgfc_status plan_create(fgfc_field field, size_t rows, size_t cols, const C* coeffs, fgfc_plan** out) {
+  if (!out || !valid_field(field)) return fail(FGFC_ERR_ARG, "Plan::matrix: invalid argument");
+  *out = nullptr;
+  size_t n;
+  if (mul_overflows(rows, cols, &n)) return fail(FGFC_ERR_OVERFLOW, "Plan::matrix: dimensions overflow");
+  if (n && !coeffs) return fail(FGFC_ERR_ARG, "Plan::matrix: null coefficients");
+  fgfc_plan* p = new fgfc_plan();
+  p->field = field;
+  p->rows = rows;
+  p->cols = cols;
+  p->values.assign(coeffs, coeffs + n);
+  for (auto& v : p->values) v &= field_mask(field);
+  p->dev = nullptr;
+  fgfc_status st = upload_plan_tables(p);
+  if (st != FGFC_OK) {
+    fgfc_plan_destroy(p);
+    return st;
+  }
+  *out = p;
+  return ok();
+}
 
 extern "C" {
 
@@ -335,29 +364,20 @@ size_t fgfc_field_bytes(fgfc_field field) { return valid_field(field) ? field_by
 
 fgfc_status fgfc_plan_create(fgfc_field field, size_t rows, size_t cols, const uint32_t* coeffs,
                              fgfc_plan** out) {
-  if (!out || !valid_field(field)) return fail(FGFC_ERR_ARG, "Plan::matrix: invalid argument");
-  *out = nullptr;
-  size_t n;
-  if (mul_overflows(rows, cols, &n)) return fail(FGFC_ERR_OVERFLOW, "Plan::matrix: dimensions overflow");
-  if (n && !coeffs) return fail(FGFC_ERR_ARG, "Plan::matrix: null coefficients");
-  fgfc_plan* p = new fgfc_plan();
-  p->field = field;
-  p->rows = rows;
-  p->cols = cols;
-  p->values.assign(coeffs, coeffs + n);
-  for (auto& v : p->values) v &= field_mask(field);
-  p->dev = nullptr;
-  fgfc_status st = upload_plan_tables(p);
-  if (st != FGFC_OK) {
-    fgfc_plan_destroy(p);
-    return st;
-  }
-  *out = p;
-  return ok();
+  return plan_create(field, rows, cols, coeffs, out);
+}
+
+fgfc_status fgfc_plan_create_u64(fgfc_field field, size_t rows, size_t cols, const uint64_t* coeffs,
+                                 fgfc_plan** out) {
+  return plan_create(field, rows, cols, coeffs, out);
 }
 
 fgfc_status fgfc_coeff_create(fgfc_field field, uint32_t coeff, fgfc_plan** out) {
-  return fgfc_plan_create(field, 1, 1, &coeff, out);
+  return plan_create(field, 1, 1, &coeff, out);
+}
+
+fgfc_status fgfc_coeff_create_u64(fgfc_field field, uint64_t coeff, fgfc_plan** out) {
+  return plan_create(field, 1, 1, &coeff, out);
 }
 
 void fgfc_plan_destroy(fgfc_plan* plan) {
@@ -387,14 +407,27 @@ fgfc_field fgfc_plan_field(const fgfc_plan* plan) {
 
 fgfc_status fgfc_plan_values(const fgfc_plan* plan, uint32_t* out) {
   if (!plan || (!out && !plan->values.empty())) return fail(FGFC_ERR_ARG, "Plan: null argument");
+  for (size_t i = 0; i < plan->values.size(); ++i) out[i] = static_cast<uint32_t>(plan->values[i]);
+  return ok();
+}
+
+fgfc_status fgfc_plan_values_u64(const fgfc_plan* plan, uint64_t* out) {
+  if (!plan || (!out && !plan->values.empty())) return fail(FGFC_ERR_ARG, "Plan: null argument");
   std::copy(plan->values.begin(), plan->values.end(), out);
+  return ok();
+}
+
+fgfc_status fgfc_plan_get_at_u64(const fgfc_plan* plan, size_t row, size_t col, uint64_t* out) {
+  if (!plan || !out) return fail(FGFC_ERR_ARG, "Plan: null argument");
+  if (row >= plan->rows || col >= plan->cols) return fail(FGFC_ERR_ARG, "Plan::get_at: out of bounds");
+  *out = plan->values[row * plan->cols + col];
   return ok();
 }
 
 fgfc_status fgfc_plan_get_at(const fgfc_plan* plan, size_t row, size_t col, uint32_t* out) {
   if (!plan || !out) return fail(FGFC_ERR_ARG, "Plan: null argument");
   if (row >= plan->rows || col >= plan->cols) return fail(FGFC_ERR_ARG, "Plan::get_at: out of bounds");
-  *out = plan->values[row * plan->cols + col];
+  *out = static_cast<uint32_t>(plan->values[row * plan->cols + col]);
   return ok();
 }
 
@@ -410,7 +443,7 @@ fgfc_status fgfc_add_assign(fgfc_field field, uint8_t* dst, size_t dst_len, cons
 }
 
 static fgfc_status mul_add_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
-                                uint32_t coeff, const fgfc_plan* plan, const uint8_t* src,
+                                uint64_t coeff, const fgfc_plan* plan, const uint8_t* src,
                                 size_t src_len, cudaStream_t stream) {
   fgfc_status st;
   if (!check_pair(field, name, "dst", dst_len, "src", src_len, &st)) return st;
@@ -459,7 +492,7 @@ fgfc_status fgfc_mul_add_with(uint8_t* dst, size_t dst_len, const fgfc_plan* coe
 }
 
 static fgfc_status mul_into_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
-                                 uint32_t coeff, const fgfc_plan* plan, const uint8_t* src,
+                                 uint64_t coeff, const fgfc_plan* plan, const uint8_t* src,
                                  size_t src_len, cudaStream_t stream) {
   fgfc_status st;
   if (!check_pair(field, name, "dst", dst_len, "src", src_len, &st)) return st;
@@ -499,7 +532,7 @@ fgfc_status fgfc_mul_into_with(uint8_t* dst, size_t dst_len, const fgfc_plan* co
 }
 
 static fgfc_status mul_assign_impl(int field, const char* name, uint8_t* dst, size_t dst_len,
-                                   uint32_t coeff, const fgfc_plan* plan, cudaStream_t stream) {
+                                   uint64_t coeff, const fgfc_plan* plan, cudaStream_t stream) {
   fgfc_status st;
   if (!check_width(field, name, dst_len, &st)) return st;
   coeff &= field_mask(field);
@@ -546,7 +579,7 @@ fgfc_status fgfc_mul_elementwise(fgfc_field field, uint8_t* dst, size_t dst_len,
 // ---------------------------------------------------------------- scatter / gather
 
 static fgfc_status scatter_impl(int field, const char* name, const char* count_word, uint8_t* rows,
-                                size_t rows_len, size_t row_len, const uint32_t* coeffs, size_t n,
+                                size_t rows_len, size_t row_len, const uint64_t* coeffs, size_t n,
                                 const fgfc_plan* plan, const uint8_t* src, size_t src_len,
                                 cudaStream_t stream) {
   fgfc_status st;
@@ -574,7 +607,7 @@ fgfc_status fgfc_mul_add_scatter(fgfc_field field, uint8_t* rows, size_t rows_le
                                  const uint32_t* coeffs, size_t ncoeffs, const uint8_t* src,
                                  size_t src_len, fgfc_stream stream) {
   if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add_scatter: unknown field");
-  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  std::vector<uint64_t> c(coeffs, coeffs + ncoeffs);
   for (auto& v : c) v &= field_mask(field);
   return scatter_impl(field, "mul_add_scatter", "coefficients", rows, rows_len, row_len, c.data(),
                       ncoeffs, nullptr, src, src_len, stream);
@@ -619,7 +652,7 @@ static bool check_sources(int field, const char* name, bool with_plan, size_t ds
 }
 
 static fgfc_status gather_impl(int field, const char* name, bool with_plan, uint8_t* dst,
-                               size_t dst_len, const uint32_t* coeffs, size_t ncoeffs,
+                               size_t dst_len, const uint64_t* coeffs, size_t ncoeffs,
                                const fgfc_plan* plan, const fgfc_slice* srcs, size_t nsrcs,
                                bool overwrite, cudaStream_t stream) {
   fgfc_status st;
@@ -651,7 +684,7 @@ fgfc_status fgfc_mul_add_gather(fgfc_field field, uint8_t* dst, size_t dst_len,
                                 const uint32_t* coeffs, size_t ncoeffs, const fgfc_slice* srcs,
                                 size_t nsrcs, fgfc_stream stream) {
   if (!valid_field(field)) return fail(FGFC_ERR_ARG, "mul_add_gather: unknown field");
-  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  std::vector<uint64_t> c(coeffs, coeffs + ncoeffs);
   for (auto& v : c) v &= field_mask(field);
   return gather_impl(field, "mul_add_gather", false, dst, dst_len, c.data(), ncoeffs, nullptr, srcs,
                      nsrcs, false, stream);
@@ -668,7 +701,7 @@ fgfc_status fgfc_dot_product(fgfc_field field, uint8_t* dst, size_t dst_len,
                              const uint32_t* coeffs, size_t ncoeffs, const fgfc_slice* srcs,
                              size_t nsrcs, fgfc_stream stream) {
   if (!valid_field(field)) return fail(FGFC_ERR_ARG, "dot_product: unknown field");
-  std::vector<uint32_t> c(coeffs, coeffs + ncoeffs);
+  std::vector<uint64_t> c(coeffs, coeffs + ncoeffs);
   for (auto& v : c) v &= field_mask(field);
   return gather_impl(field, "dot_product", false, dst, dst_len, c.data(), ncoeffs, nullptr, srcs, nsrcs,
                      true, stream);
@@ -712,7 +745,7 @@ static fgfc_status matrix_terms_impl(int field, const char* name, bool overwrite
     }
     return ok();
   }
-  std::vector<uint32_t> coeffs(nterms * nrows);
+  std::vector<uint64_t> coeffs(nterms * nrows);
   std::vector<const uint8_t*> sp(nterms);
   for (size_t t = 0; t < nterms; ++t) {
     sp[t] = terms[t].src;
@@ -848,7 +881,7 @@ fgfc_status fgfc_mul_add_matrix_scattered(fgfc_field field, uint8_t* dst, size_t
                   row_len);
   }
   if (nrows == 0 || nterms == 0) return ok();
-  std::vector<uint32_t> coeffs(nterms * nrows);
+  std::vector<uint64_t> coeffs(nterms * nrows);
   std::vector<const uint8_t*> sp(nterms);
   for (size_t t = 0; t < nterms; ++t) {
     sp[t] = terms[t].src;
@@ -1080,6 +1113,19 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
       }
       continue;
     }
+    if (field_bytes(field) == 8) {  // 8-byte fields have their own kernel: one launch per stripe
+      std::vector<uint8_t*> rp(J.nrows);
+      for (size_t j = 0; j < J.nrows; ++j) rp[j] = J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len);
+      std::vector<const uint8_t*> sp(J.nsrcs);
+      for (size_t t = 0; t < J.nsrcs; ++t) sp[t] = J.srcs[t].ptr;
+      st = run_matrix(field, sp.data(), J.nsrcs, rp.data(), J.nrows, plan_mat(plan), J.row_len, J.overwrite != 0,
+                      stream, name);
+      if (st != FGFC_OK) {
+        t_err = "batch job " + std::to_string(i) + ": " + t_err;
+        return st;
+      }
+      continue;
+    }
     std::vector<uint64_t> dsts(J.nrows);
     for (size_t j = 0; j < J.nrows; ++j)
       dsts[j] = reinterpret_cast<uint64_t>(J.dst + (J.row_starts ? J.row_starts[j] : j * J.row_len));
@@ -1120,6 +1166,9 @@ fgfc_status fgfc_run_jobs_serial(const fgfc_matrix_job* jobs, size_t njobs, fgfc
 fgfc_status fgfc_batch_run_noalloc(fgfc_field field, const fgfc_noalloc_job* jobs, size_t njobs,
                                    fgfc_stream stream) {
   if (!valid_field(field) || (njobs && !jobs)) return fail(FGFC_ERR_ARG, "batch_run_noalloc: invalid argument");
+  if (field_bytes(field) > 4)
+    return fail(FGFC_ERR_LIMIT, "batch_run_noalloc: %s has 8-byte elements; this entry point takes 1-, 2- and "
+                "4-byte fields", field_name(field));
   for (size_t i = 0; i < njobs; ++i) {
     const fgfc_noalloc_job& J = jobs[i];
     const char* name =

@@ -1296,7 +1296,7 @@ int noalloc_run(int field, const fgfc_noalloc_job* jobs, size_t njobs, cudaStrea
       J.head = std::min<uint64_t>((16 - al) & 15, S.row_len);
       J.nvec = (S.row_len - J.head) / 16;
     }
-    uint32_t cm[kMaxSrc * 16];  // coefficients reduced to the field's width, as Plan::matrix does
+    uint64_t cm[kMaxSrc * 16];  // coefficients reduced to the field's width, as Plan::matrix does
     for (size_t q = 0; q < S.nsrcs * S.nrows; ++q) cm[q] = S.coeffs[q] & field_mask(field);
     build_compact_tables(field, cm, S.nrows, 0, S.nsrcs, 0, G, ht + tn);
     J.tables = reinterpret_cast<const uint32_t*>(dbase + off_tabs) + tn;

@@ -65,6 +65,9 @@ fgfc_status decode_matrix(int field, const uint32_t* parity, size_t k, size_t m,
                           const size_t* erased, size_t nerased, uint32_t* out) {
   const char* name = "decode_matrix";
   if (field_bytes(field) == 0) return set_error(FGFC_ERR_ARG, "decode_matrix: unknown field");
+  if (field_bytes(field) > 4)
+    return set_error(FGFC_ERR_ARG, "decode_matrix: 8-byte fields need 64-bit coefficients, which these 32-bit "
+                                   "arrays cannot hold");
   if (!k || (m && !parity) || !survivors || (nerased && (!erased || !out)))
     return set_error(FGFC_ERR_ARG, "decode_matrix: null argument");
   const uint32_t mask = field_mask(field);
@@ -105,6 +108,9 @@ extern "C" {
 
 fgfc_status fgfc_cauchy_matrix(fgfc_field field, size_t m, size_t k, uint32_t x0, uint32_t* out) {
   if (field_bytes(field) == 0 || (m * k && !out)) return set_error(FGFC_ERR_ARG, "cauchy_matrix: invalid argument");
+  if (field_bytes(field) > 4)
+    return set_error(FGFC_ERR_ARG, "cauchy_matrix: 8-byte fields need 64-bit coefficients, which these 32-bit "
+                                   "arrays cannot hold");
   for (size_t i = 0; i < m; ++i)
     for (size_t j = 0; j < k; ++j) {
       const uint32_t x = static_cast<uint32_t>(x0 + i), y = static_cast<uint32_t>(j);

@@ -630,23 +630,23 @@ __global__ void __launch_bounds__(kMmaThreads, 1) gf2mma_kernel(const __grid_con
 
 bool gf2mma_shape_ok(int field, size_t k, size_t m) {
   const int E = field_bytes(field);
-  return E > 0 && k >= 1 && m >= 1 && k * E <= kMaxInBits / 8 && m * E <= kMaxOutBits / 8;
+  return E > 0 && E <= 4 && k >= 1 && m >= 1 && k * E <= kMaxInBits / 8 && m * E <= kMaxOutBits / 8;
 }
 
 // Bit matrix of a coefficient matrix (term-major, k x m): bits[n][g] bit
 // (8r + b) = output bit n (byte n / 8 of the m*E output bytes, bit n % 8)
 // depends on bit b of input byte 4g + r (input byte u = t * E + p).
-void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t* bits /* [128][16] */) {
+void gf2mma_bits(int field, const uint64_t* coeffs, size_t k, size_t m, uint32_t* bits /* [128][16] */) {
   const int E = field_bytes(field);
   std::memset(bits, 0, kMaxOutBits * (kMaxInBits / 32) * sizeof(uint32_t));
   for (size_t t = 0; t < k; ++t)
     for (size_t j = 0; j < m; ++j) {
-      uint32_t img[4][8];
+      uint64_t img[8][8];
       coeff_images(field, coeffs[t * m + j], img);
       for (int p = 0; p < E; ++p) {
         const size_t u = t * E + p;
         for (int b = 0; b < 8; ++b) {
-          const uint32_t prod = img[p][b];  // c * (bit b of input byte p), E bytes
+          const uint64_t prod = img[p][b];  // c * (bit b of input byte p), E bytes
           for (int ob = 0; ob < 8 * E; ++ob)
             if ((prod >> ob) & 1u) {
               const size_t n = j * E * 8 + ob;

@@ -48,7 +48,7 @@ struct MatrixLaunch {
 // Build compact tables for sources [t0, t0+k) and groups [g0, g0+G) of a
 // coefficient matrix (term-major: coeffs[t * m + j]). Output layout
 // [(t * E + p) * G + g][32].
-void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0, size_t k,
+void build_compact_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k,
                           size_t g0, size_t G, uint32_t* out);
 
 // Kernel entry (kernels.cu). `groups` = G for this launch; `overwrite`
@@ -77,7 +77,7 @@ bool gf2mma_shape_ok(int field, size_t k, size_t m);
 // Compact GF(2) bit matrix of a term-major k x m coefficient matrix:
 // kGf2BitWords words, [output bit][input word group].
 constexpr size_t kGf2BitWords = 128 * 16;
-void gf2mma_bits(int field, const uint32_t* coeffs, size_t k, size_t m, uint32_t* bits);
+void gf2mma_bits(int field, const uint64_t* coeffs, size_t k, size_t m, uint32_t* bits);
 // Columns [0, nblk * 512 * E) of k sources and m rows, all 16-byte aligned.
 cudaError_t gf2mma_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
                           const uint32_t* bits, uint64_t nblk, bool overwrite, cudaStream_t stream);
@@ -135,6 +135,14 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
 // shares one offset within 16 bytes) plus table sub-jobs for the rest.
 void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, const std::vector<uint64_t>& dsts,
                       size_t row_len, bool overwrite, std::vector<LoweredJob>& out, std::vector<Gf2Job>& tc);
+
+// The matrix ops for 8-byte fields (wide.cu): coefficients either as raw
+// host values (term-major k x m, tables built into the launch parameters) or
+// as a plan's device tables in the compact layout with `gstride` groups per
+// (source, byte plane).
+cudaError_t wide_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
+                        const uint64_t* host_coeffs, const uint32_t* dev_tables, size_t gstride, size_t len,
+                        bool overwrite, cudaStream_t stream);
 
 // Error text of the calling thread (api.cpp), for entry points defined in
 // other files.

@@ -491,7 +491,7 @@ __global__ void elementwise_kernel(uint8_t* __restrict__ dst, const uint8_t* __r
 
 // ---- mul_elementwise over the Fan-Paar towers. Byte products use the
 // byte level's log/exp tables (generator 0x2d) and a byte times the byte
-// level's top generator alpha uses a 256-entry table; the 16- and 32-bit
+// level's top generator alpha uses a 256-entry table; the 16-, 32- and 64-bit
 // levels follow the Karatsuba recursion of the tower X^2 + alpha X + 1
 // (src/field/fan_paar.rs:80-94, 122-134). Tables: 1 KiB, staged from
 // constant memory into shared memory per CTA.
@@ -517,6 +517,15 @@ struct FpTab {
     const uint32_t z0 = m16(a0, b0), z2 = m16(a1, b1), z1 = m16(a0 ^ a1, b0 ^ b1) ^ z0 ^ z2;
     return (z0 ^ z2) | ((z1 ^ alpha16(z2)) << 16);
   }
+  __device__ __forceinline__ uint32_t alpha32(uint32_t v) const {  // v * alpha at the 32-bit level
+    return (v >> 16) | (((v & 0xFFFFu) ^ alpha16(v >> 16)) << 16);
+  }
+  __device__ __forceinline__ uint64_t m64(uint64_t x, uint64_t y) const {
+    const uint32_t a0 = static_cast<uint32_t>(x), a1 = static_cast<uint32_t>(x >> 32);
+    const uint32_t b0 = static_cast<uint32_t>(y), b1 = static_cast<uint32_t>(y >> 32);
+    const uint32_t z0 = m32(a0, b0), z2 = m32(a1, b1), z1 = m32(a0 ^ a1, b0 ^ b1) ^ z0 ^ z2;
+    return static_cast<uint64_t>(z0 ^ z2) | (static_cast<uint64_t>(z1 ^ alpha32(z2)) << 32);
+  }
 };
 
 template <int E>
@@ -528,15 +537,41 @@ __global__ void elementwise_fp_kernel(uint8_t* __restrict__ dst, const uint8_t* 
   const FpTab T{tab, tab + 512, tab + 768};
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem; i += stride) {
-    uint32_t x = 0, y = 0;
+    uint64_t x = 0, y = 0;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      x |= static_cast<uint32_t>(a[E * i + k]) << (8 * k);
-      y |= static_cast<uint32_t>(b[E * i + k]) << (8 * k);
+      x |= static_cast<uint64_t>(a[E * i + k]) << (8 * k);
+      y |= static_cast<uint64_t>(b[E * i + k]) << (8 * k);
     }
-    const uint32_t r = E == 1 ? T.m8(x, y) : (E == 2 ? T.m16(x, y) : T.m32(x, y));
+    const uint64_t r = E == 1   ? T.m8(static_cast<uint32_t>(x), static_cast<uint32_t>(y))
+                       : E == 2 ? T.m16(static_cast<uint32_t>(x), static_cast<uint32_t>(y))
+                       : E == 4 ? T.m32(static_cast<uint32_t>(x), static_cast<uint32_t>(y))
+                                : T.m64(x, y);
 #pragma unroll
     for (int k = 0; k < E; ++k) dst[E * i + k] = static_cast<uint8_t>(r >> (8 * k));
+  }
+}
+
+// GF(2^64) = Gf32[w]/(w^2 + w + 0x20000000): three word-parallel Gf32
+// products and one product by the constant (src/field/gf64.rs:120-128).
+__global__ void elementwise_gf64_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ a,
+                                        const uint8_t* __restrict__ b, uint64_t nelem) {
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem; i += stride) {
+    uint64_t x = 0, y = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      x |= static_cast<uint64_t>(a[8 * i + k]) << (8 * k);
+      y |= static_cast<uint64_t>(b[8 * i + k]) << (8 * k);
+    }
+    const uint32_t p = static_cast<uint32_t>(x), q = static_cast<uint32_t>(x >> 32);
+    const uint32_t c = static_cast<uint32_t>(y), d = static_cast<uint32_t>(y >> 32);
+    const uint32_t ac = gmul32(p, c), bd = gmul32(q, d);
+    const uint32_t lo = ac ^ gmul32(bd, 0x20000000u);
+    const uint32_t hi = gmul32(p ^ q, c ^ d) ^ ac;
+    const uint64_t r = static_cast<uint64_t>(lo) | (static_cast<uint64_t>(hi) << 32);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dst[8 * i + k] = static_cast<uint8_t>(r >> (8 * k));
   }
 }
 
@@ -641,8 +676,10 @@ static cudaError_t launch_elementwise_fp(int field, uint8_t* dst, const uint8_t*
     elementwise_fp_kernel<1><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
   else if (E == 2)
     elementwise_fp_kernel<2><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
-  else
+  else if (E == 4)
     elementwise_fp_kernel<4><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
+  else
+    elementwise_fp_kernel<8><<<blocks, 256, 0, s>>>(dst, a, b, nelem);
   return cudaGetLastError();
 }
 
@@ -651,7 +688,14 @@ cudaError_t launch_elementwise(int field, uint8_t* dst, const uint8_t* a, const 
   if (!len) return cudaSuccess;
   const int E = field_bytes(field);
   if (E <= 0 || len % E) return cudaErrorInvalidValue;
-  if (field == kFp8 || field == kFp16 || field == kFp32) return launch_elementwise_fp(field, dst, a, b, len, s);
+  if (field == kFp8 || field == kFp16 || field == kFp32 || field == kFp64)
+    return launch_elementwise_fp(field, dst, a, b, len, s);
+  if (field == kGf64) {
+    const uint64_t nelem = len / 8;
+    uint64_t want = (nelem + 255) / 256, cap = static_cast<uint64_t>(sm_count()) * 8;
+    elementwise_gf64_kernel<<<static_cast<unsigned>(want < cap ? want : cap), 256, 0, s>>>(dst, a, b, nelem);
+    return cudaGetLastError();
+  }
   const uint64_t ad = reinterpret_cast<uintptr_t>(dst) & 15;
   uint64_t head = len, nvec = 0;
   if (ad == (reinterpret_cast<uintptr_t>(a) & 15) && ad == (reinterpret_cast<uintptr_t>(b) & 15)) {

@@ -754,6 +754,9 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
   fgfc_status st = validate_matrix_call(q->field, name, q->dst_len, q->row_len, q->row_starts, q->nrows, q->srcs,
                                         q->nsrcs, q->coeffs, q->overwrite);
   if (st != FGFC_OK) return st;
+  if (field_bytes(q->field) > 4)
+    return set_error(FGFC_ERR_ARG, "server: 8-byte fields are not served (their coefficients do not fit the "
+                                   "request's 32-bit coefficient array)");
   auto r = std::make_unique<Req>();
   r->field = q->field;
   r->k = q->nsrcs;
@@ -837,6 +840,9 @@ fgfc_status fgfc_server_submit(fgfc_server* s, const fgfc_request* q, uint64_t* 
 fgfc_status fgfc_server_submit_rebuild(fgfc_server* s, const fgfc_rebuild_request* q, uint64_t* ticket) {
   if (!s || !q || !ticket) return set_error(FGFC_ERR_ARG, "server: null argument");
   if (field_bytes(q->field) == 0) return set_error(FGFC_ERR_ARG, "server: unknown field");
+  if (field_bytes(q->field) > 4)
+    return set_error(FGFC_ERR_ARG, "server: 8-byte fields are not served (their coefficients do not fit the "
+                                   "request's 32-bit coefficient arrays)");
   if (!q->k || !q->survivors || !q->parity || (q->nerased && !q->erased))
     return set_error(FGFC_ERR_ARG, "server: rebuild request without code or pattern");
   uint64_t h = 0xcbf29ce484222325ull;

@@ -14,22 +14,31 @@ const Gf8Log& gf8d_tab() {
   return t;
 }
 
-void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0, size_t k,
+void build_compact_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k,
                           size_t g0, size_t G, uint32_t* out) {
   const int E = field_bytes(field);
-  const int R = 4 / E;
   for (size_t tt = 0; tt < k; ++tt) {
     const size_t t = t0 + tt;
     for (size_t g = 0; g < G; ++g) {
-      // Images of the R coefficients this group covers (rows past m
-      // contribute zero products).
-      uint32_t img[4][4][8];
-      for (int r = 0; r < R; ++r) {
-        const size_t j = (g0 + g) * R + r;
-        if (j < m) {
-          coeff_images(field, coeffs[t * m + j], img[r]);
-        } else {
-          std::memset(img[r], 0, sizeof img[r]);
+      // The group's 4 output bytes are the flat output bytes
+      // f = 4 (g0 + g) + q of the m * E (row f / E, byte f % E); rows past m
+      // contribute zero products. Images per row this group touches.
+      uint64_t img[4][8][8];
+      size_t row[4];
+      int ri[4], ob[4];
+      int nr = 0;
+      for (int q = 0; q < 4; ++q) {
+        const size_t f = 4 * (g0 + g) + q;
+        const size_t j = f / E;
+        ob[q] = static_cast<int>(f % E);
+        ri[q] = -1;
+        if (j >= m) continue;
+        for (int r = 0; r < nr; ++r)
+          if (row[r] == j) ri[q] = r;
+        if (ri[q] < 0) {
+          row[nr] = j;
+          coeff_images(field, coeffs[t * m + j], img[nr]);
+          ri[q] = nr++;
         }
       }
       for (int p = 0; p < E; ++p) {
@@ -39,7 +48,7 @@ void build_compact_tables(int field, const uint32_t* coeffs, size_t m, size_t t0
             const uint8_t x = static_cast<uint8_t>(half ? (n << 4) : n);
             uint32_t word = 0;
             for (int q = 0; q < 4; ++q)
-              word |= static_cast<uint32_t>(image_byte(img[q / E], p, x, q % E)) << (8 * q);
+              if (ri[q] >= 0) word |= static_cast<uint32_t>(image_byte(img[ri[q]], p, x, ob[q])) << (8 * q);
             slot[half * 16 + n] = word;
           }
       }

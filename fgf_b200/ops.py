@@ -66,6 +66,18 @@ def _u32s(values: Iterable[int]):
     return (C.c_uint32 * max(1, len(vals)))(*vals), len(vals)
 
 
+def _u64s(values: Iterable[int]):
+    vals = [int(v) & 0xFFFFFFFFFFFFFFFF for v in values]
+    return (C.c_uint64 * max(1, len(vals)))(*vals), len(vals)
+
+
+def _wide(field) -> bool:
+    """8-byte fields: their coefficients are 64-bit, so the raw forms below
+    prepare a plan and run the prepared form (the C ABI's raw entry points
+    take 32-bit coefficients)."""
+    return FIELDS[_fid(field)].BYTES == 8
+
+
 def _slices(srcs: Sequence) -> tuple[C.Array, int]:
     bufs = [_buf(s) for s in srcs]
     arr = (Slice * max(1, len(bufs)))(*[Slice(p, n) for p, n in bufs])
@@ -99,9 +111,9 @@ class Plan:
         vals = [int(v) for v in coeffs]
         rows = 1 if _rows is None else _rows
         cols = len(vals) if _cols is None else _cols
-        arr, _ = _u32s(vals)
+        arr, _ = _u64s(vals)
         h = C.c_void_p()
-        check(lib().fgfc_plan_create(self.field.ID, rows, cols, arr, C.byref(h)))
+        check(lib().fgfc_plan_create_u64(self.field.ID, rows, cols, arr, C.byref(h)))
         self._h = h
         self._values = [v & ((1 << (8 * self.field.BYTES)) - 1) for v in vals]
         self._rows, self._cols = rows, cols
@@ -116,8 +128,8 @@ class Plan:
         self = cls.__new__(cls)
         self.field = FIELDS[_fid(field)]
         self._h = handle
-        vals = (C.c_uint32 * max(1, rows * cols))()
-        check(lib().fgfc_plan_values(handle, vals))
+        vals = (C.c_uint64 * max(1, rows * cols))()
+        check(lib().fgfc_plan_values_u64(handle, vals))
         self._values = list(vals[:rows * cols])
         self._rows, self._cols = rows, cols
         return self
@@ -231,6 +243,8 @@ def sub_assign(field, dst, src, stream=None) -> None:
 
 def mul_add(field, dst, coeff: int, src, stream=None) -> None:
     """`dst ^= coeff * src` (src/ops.rs:342-352)."""
+    if _wide(field):
+        return mul_add_with(dst, Coeff(field, coeff), src, stream)
     d, dn = _buf(dst)
     s, sn = _buf(src)
     check(lib().fgfc_mul_add(_fid(field), d, dn, int(coeff) & 0xFFFFFFFF, s, sn, _stream(stream)))
@@ -248,6 +262,8 @@ def mul_add_with(dst, coeff, src, stream=None) -> None:
 
 def mul_into(field, dst, coeff: int, src, stream=None) -> None:
     """`dst = coeff * src` (src/ops.rs:381-392)."""
+    if _wide(field):
+        return mul_into_with(dst, Coeff(field, coeff), src, stream)
     d, dn = _buf(dst)
     s, sn = _buf(src)
     check(lib().fgfc_mul_into(_fid(field), d, dn, int(coeff) & 0xFFFFFFFF, s, sn, _stream(stream)))
@@ -265,6 +281,8 @@ def mul_into_with(dst, coeff, src, stream=None) -> None:
 
 def mul_assign(field, dst, coeff: int, stream=None) -> None:
     """`dst *= coeff` in place (src/ops.rs:422-432)."""
+    if _wide(field):
+        return mul_assign_with(dst, Coeff(field, coeff), stream)
     d, dn = _buf(dst)
     check(lib().fgfc_mul_assign(_fid(field), d, dn, int(coeff) & 0xFFFFFFFF, _stream(stream)))
 
@@ -290,6 +308,8 @@ def mul_elementwise(field, dst, a, b, stream=None) -> None:
 
 def mul_add_scatter(field, rows, row_len: int, coeffs: Sequence[int], src, stream=None) -> None:
     """`rows[j] ^= coeffs[j] * src` (src/ops.rs:461-482)."""
+    if _wide(field) and len(coeffs):
+        return mul_add_scatter_with(rows, row_len, Plan.new(field, coeffs), src, stream)
     r, rn = _buf(rows)
     s, sn = _buf(src)
     arr, n = _u32s(coeffs)
@@ -305,6 +325,8 @@ def mul_add_scatter_with(rows, row_len: int, plan: Plan, src, stream=None) -> No
 
 def mul_add_gather(field, dst, coeffs: Sequence[int], srcs: Sequence, stream=None) -> None:
     """`dst ^= sum coeffs[i] * srcs[i]` (src/ops.rs:533-555)."""
+    if _wide(field) and len(coeffs) and len(coeffs) == len(srcs):
+        return mul_add_gather_with(dst, Plan.new(field, coeffs), srcs, stream)
     d, dn = _buf(dst)
     arr, n = _u32s(coeffs)
     sl, ns = _slices(srcs)
@@ -320,6 +342,8 @@ def mul_add_gather_with(dst, plan: Plan, srcs: Sequence, stream=None) -> None:
 
 def dot_product(field, dst, coeffs: Sequence[int], srcs: Sequence, stream=None) -> None:
     """`dst = sum coeffs[i] * srcs[i]` (src/ops.rs:597-624)."""
+    if _wide(field) and len(coeffs) and len(coeffs) == len(srcs):
+        return dot_product_with(dst, Plan.new(field, coeffs), srcs, stream)
     d, dn = _buf(dst)
     arr, n = _u32s(coeffs)
     sl, ns = _slices(srcs)
@@ -337,6 +361,9 @@ def dot_product_with(dst, plan: Plan, srcs: Sequence, stream=None) -> None:
 
 def mul_add_matrix(field, rows, row_len: int, nrows: int, terms: Sequence, stream=None) -> None:
     """`rows[j] ^= sum_t coeffs_t[j] * src_t` over `(coeffs, src)` terms (src/ops.rs:675-708)."""
+    if _wide(field) and terms and all(len(c) == nrows for c, _ in terms):
+        plan = Plan.matrix(field, len(terms), nrows, [int(v) for c, _ in terms for v in c])
+        return mul_add_matrix_with(rows, row_len, nrows, plan, [src for _, src in terms], stream)
     r, rn = _buf(rows)
     arr, n, _keep = _terms(terms)
     check(lib().fgfc_mul_add_matrix(_fid(field), r, rn, row_len, nrows, arr, n, _stream(stream)))
@@ -351,6 +378,9 @@ def mul_add_matrix_with(rows, row_len: int, nrows: int, plan: Plan, srcs: Sequen
 
 def dot_product_matrix(field, rows, row_len: int, nrows: int, terms: Sequence, stream=None) -> None:
     """Overwrite form of mul_add_matrix (src/ops.rs:773-810)."""
+    if _wide(field) and terms and all(len(c) == nrows for c, _ in terms):
+        plan = Plan.matrix(field, len(terms), nrows, [int(v) for c, _ in terms for v in c])
+        return dot_product_matrix_with(rows, row_len, nrows, plan, [src for _, src in terms], stream)
     r, rn = _buf(rows)
     arr, n, _keep = _terms(terms)
     check(lib().fgfc_dot_product_matrix(_fid(field), r, rn, row_len, nrows, arr, n, _stream(stream)))
@@ -367,6 +397,9 @@ def dot_product_matrix_with(rows, row_len: int, nrows: int, plan: Plan, srcs: Se
 def mul_add_matrix_scattered(field, dst, row_len: int, row_starts: Sequence[int], terms: Sequence,
                              stream=None) -> None:
     """Rows at dst[row_starts[j]..] (src/ops.rs:887-941)."""
+    if _wide(field) and terms and all(len(c) == len(row_starts) for c, _ in terms):
+        plan = Plan.matrix(field, len(terms), len(row_starts), [int(v) for c, _ in terms for v in c])
+        return mul_add_matrix_scattered_with(dst, row_len, row_starts, plan, [src for _, src in terms], stream)
     d, dn = _buf(dst)
     starts = (C.c_size_t * max(1, len(row_starts)))(*[int(s) for s in row_starts])
     arr, n, _keep = _terms(terms)

@@ -9,91 +9,118 @@
 use std::marker::PhantomData;
 use std::ptr;
 
-use fgf::fan_paar::{fp16, fp32, fp8, FanPaar16, FanPaar32, FanPaar8};
-use fgf::field::{gf16, gf32, gf8b, gf8d, Field, Gf16, Gf32, Gf8B, Gf8D};
+use fgf::fan_paar::{fp16, fp32, fp64, fp8, FanPaar16, FanPaar32, FanPaar64, FanPaar8};
+use fgf::field::{gf16, gf32, gf64, gf8b, gf8d, Field, Gf16, Gf32, Gf64, Gf8B, Gf8D};
 
 use crate::device::{DeviceSlice, DeviceSliceMut, Stream};
 use crate::{check, sys};
 
-/// A field the device library implements: its ABI code and element <-> u32.
+/// A field the device library implements: its ABI code and element <-> u64.
+/// `WIDE` marks the 8-byte fields, whose 64-bit coefficients reach the
+/// library only through plans (the raw entry points take 32-bit values).
 pub trait CudaField: Field {
     const ID: sys::fgfc_field;
-    fn to_raw(e: Self::Elem) -> u32;
-    fn from_raw(v: u32) -> Self::Elem;
+    const WIDE: bool = false;
+    fn to_raw(e: Self::Elem) -> u64;
+    fn from_raw(v: u64) -> Self::Elem;
 }
 
 impl CudaField for Gf8B {
     const ID: sys::fgfc_field = sys::FGFC_GF8B;
-    fn to_raw(e: gf8b::Elem) -> u32 {
-        u32::from(e.0)
+    fn to_raw(e: gf8b::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> gf8b::Elem {
+    fn from_raw(v: u64) -> gf8b::Elem {
         gf8b::Elem(v as u8)
     }
 }
 
 impl CudaField for Gf8D {
     const ID: sys::fgfc_field = sys::FGFC_GF8D;
-    fn to_raw(e: gf8d::Elem) -> u32 {
-        u32::from(e.0)
+    fn to_raw(e: gf8d::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> gf8d::Elem {
+    fn from_raw(v: u64) -> gf8d::Elem {
         gf8d::Elem(v as u8)
     }
 }
 
 impl CudaField for Gf16 {
     const ID: sys::fgfc_field = sys::FGFC_GF16;
-    fn to_raw(e: gf16::Elem) -> u32 {
-        u32::from(e.0)
+    fn to_raw(e: gf16::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> gf16::Elem {
+    fn from_raw(v: u64) -> gf16::Elem {
         gf16::Elem(v as u16)
     }
 }
 
 impl CudaField for Gf32 {
     const ID: sys::fgfc_field = sys::FGFC_GF32;
-    fn to_raw(e: gf32::Elem) -> u32 {
-        e.0
+    fn to_raw(e: gf32::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> gf32::Elem {
-        gf32::Elem(v)
+    fn from_raw(v: u64) -> gf32::Elem {
+        gf32::Elem(v as u32)
     }
 }
 
 impl CudaField for FanPaar8 {
     const ID: sys::fgfc_field = sys::FGFC_FP8;
-    fn to_raw(e: fp8::Elem) -> u32 {
-        u32::from(e.0)
+    fn to_raw(e: fp8::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> fp8::Elem {
+    fn from_raw(v: u64) -> fp8::Elem {
         fp8::Elem(v as u8)
     }
 }
 
 impl CudaField for FanPaar16 {
     const ID: sys::fgfc_field = sys::FGFC_FP16;
-    fn to_raw(e: fp16::Elem) -> u32 {
-        u32::from(e.0)
+    fn to_raw(e: fp16::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> fp16::Elem {
+    fn from_raw(v: u64) -> fp16::Elem {
         fp16::Elem(v as u16)
     }
 }
 
 impl CudaField for FanPaar32 {
     const ID: sys::fgfc_field = sys::FGFC_FP32;
-    fn to_raw(e: fp32::Elem) -> u32 {
-        e.0
+    fn to_raw(e: fp32::Elem) -> u64 {
+        u64::from(e.0)
     }
-    fn from_raw(v: u32) -> fp32::Elem {
-        fp32::Elem(v)
+    fn from_raw(v: u64) -> fp32::Elem {
+        fp32::Elem(v as u32)
     }
 }
 
+impl CudaField for Gf64 {
+    const ID: sys::fgfc_field = sys::FGFC_GF64;
+    const WIDE: bool = true;
+    fn to_raw(e: gf64::Elem) -> u64 {
+        e.0
+    }
+    fn from_raw(v: u64) -> gf64::Elem {
+        gf64::Elem(v)
+    }
+}
+
+impl CudaField for FanPaar64 {
+    const ID: sys::fgfc_field = sys::FGFC_FP64;
+    const WIDE: bool = true;
+    fn to_raw(e: fp64::Elem) -> u64 {
+        e.0
+    }
+    fn from_raw(v: u64) -> fp64::Elem {
+        fp64::Elem(v)
+    }
+}
+
+/// 32-bit coefficients for the raw entry points (every field but the 8-byte
+/// ones, whose raw forms below go through a plan).
 fn raw<F: CudaField>(coeffs: &[F::Elem]) -> Vec<u32> {
-    coeffs.iter().map(|&c| F::to_raw(c)).collect()
+    coeffs.iter().map(|&c| F::to_raw(c) as u32).collect()
 }
 
 fn stream() -> sys::fgfc_stream {
@@ -134,17 +161,17 @@ impl<F: CudaField> Plan<F> {
     pub fn matrix(rows: usize, cols: usize, coeffs: &[F::Elem]) -> Self {
         let expected = rows.checked_mul(cols).expect("Plan::matrix: dimensions overflow");
         assert_eq!(coeffs.len(), expected, "Plan::matrix: {} coefficients for {rows}x{cols} matrix", coeffs.len());
-        let v = raw::<F>(coeffs);
+        let v: Vec<u64> = coeffs.iter().map(|&c| F::to_raw(c)).collect();
         let mut p = ptr::null_mut();
         // SAFETY: v holds rows * cols values; p receives a new plan.
-        check(unsafe { sys::fgfc_plan_create(F::ID, rows, cols, v.as_ptr(), &mut p) });
+        check(unsafe { sys::fgfc_plan_create_u64(F::ID, rows, cols, v.as_ptr(), &mut p) });
         Self { raw: p, values: coeffs.to_vec(), rows, cols, _f: PhantomData }
     }
 
     pub(crate) fn adopt(raw: *mut sys::fgfc_plan, rows: usize, cols: usize) -> Self {
-        let mut v = vec![0u32; rows * cols];
+        let mut v = vec![0u64; rows * cols];
         // SAFETY: the plan holds rows * cols values.
-        check(unsafe { sys::fgfc_plan_values(raw, v.as_mut_ptr()) });
+        check(unsafe { sys::fgfc_plan_values_u64(raw, v.as_mut_ptr()) });
         Self { raw, values: v.into_iter().map(F::from_raw).collect(), rows, cols, _f: PhantomData }
     }
 
@@ -261,8 +288,11 @@ pub fn sub_assign<F: CudaField>(dst: &mut DeviceSliceMut<'_>, src: &DeviceSlice<
 /// `ops::mul_add` (src/ops.rs:342): `dst ^= coeff * src`.
 #[track_caller]
 pub fn mul_add<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeff: F::Elem, src: &DeviceSlice<'_>) {
+    if F::WIDE {
+        return mul_add_with(dst, &Coeff::<F>::new(coeff), src);
+    }
     check(unsafe {
-        sys::fgfc_mul_add(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff), src.as_ptr(), src.len(), stream())
+        sys::fgfc_mul_add(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff) as u32, src.as_ptr(), src.len(), stream())
     });
 }
 
@@ -276,8 +306,11 @@ pub fn mul_add_with<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeff: &impl Pre
 /// `ops::mul_into` (src/ops.rs:381): `dst = coeff * src`.
 #[track_caller]
 pub fn mul_into<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeff: F::Elem, src: &DeviceSlice<'_>) {
+    if F::WIDE {
+        return mul_into_with(dst, &Coeff::<F>::new(coeff), src);
+    }
     check(unsafe {
-        sys::fgfc_mul_into(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff), src.as_ptr(), src.len(), stream())
+        sys::fgfc_mul_into(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff) as u32, src.as_ptr(), src.len(), stream())
     });
 }
 
@@ -291,7 +324,10 @@ pub fn mul_into_with<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeff: &impl Pr
 /// `ops::mul_assign` (src/ops.rs:422): `dst *= coeff`.
 #[track_caller]
 pub fn mul_assign<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeff: F::Elem) {
-    check(unsafe { sys::fgfc_mul_assign(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff), stream()) });
+    if F::WIDE {
+        return mul_assign_with(dst, &Coeff::<F>::new(coeff));
+    }
+    check(unsafe { sys::fgfc_mul_assign(F::ID, dst.as_mut_ptr(), dst.len(), F::to_raw(coeff) as u32, stream()) });
 }
 
 /// `ops::mul_assign_with` (src/ops.rs:439).
@@ -314,6 +350,9 @@ pub fn mul_elementwise<F: CudaField>(dst: &mut DeviceSliceMut<'_>, a: &DeviceSli
 /// `ops::mul_add_scatter` (src/ops.rs:461): `rows[j] ^= coeffs[j] * src`.
 #[track_caller]
 pub fn mul_add_scatter<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_len: usize, coeffs: &[F::Elem], src: &DeviceSlice<'_>) {
+    if F::WIDE && !coeffs.is_empty() {
+        return mul_add_scatter_with(rows, row_len, &Plan::<F>::new(coeffs), src);
+    }
     let c = raw::<F>(coeffs);
     check(unsafe {
         sys::fgfc_mul_add_scatter(F::ID, rows.as_mut_ptr(), rows.len(), row_len, c.as_ptr(), c.len(), src.as_ptr(),
@@ -332,6 +371,9 @@ pub fn mul_add_scatter_with<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_len
 /// `ops::mul_add_gather` (src/ops.rs:533): `dst ^= sum coeffs[i] * srcs[i]`.
 #[track_caller]
 pub fn mul_add_gather<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeffs: &[F::Elem], srcs: &[DeviceSlice<'_>]) {
+    if F::WIDE && !coeffs.is_empty() && coeffs.len() == srcs.len() {
+        return mul_add_gather_with(dst, &Plan::<F>::new(coeffs), srcs);
+    }
     let c = raw::<F>(coeffs);
     let s = slices(srcs);
     check(unsafe {
@@ -349,6 +391,9 @@ pub fn mul_add_gather_with<F: CudaField>(dst: &mut DeviceSliceMut<'_>, plan: &Pl
 /// `ops::dot_product` (src/ops.rs:597): `dst = sum coeffs[i] * srcs[i]`.
 #[track_caller]
 pub fn dot_product<F: CudaField>(dst: &mut DeviceSliceMut<'_>, coeffs: &[F::Elem], srcs: &[DeviceSlice<'_>]) {
+    if F::WIDE && !coeffs.is_empty() && coeffs.len() == srcs.len() {
+        return dot_product_with(dst, &Plan::<F>::new(coeffs), srcs);
+    }
     let c = raw::<F>(coeffs);
     let s = slices(srcs);
     check(unsafe {
@@ -365,6 +410,18 @@ pub fn dot_product_with<F: CudaField>(dst: &mut DeviceSliceMut<'_>, plan: &Plan<
 
 // ---------------------------------------------------------------- many-to-many
 
+/// For an 8-byte field: the terms as a (sources, rows) plan and their
+/// sources, when every term carries `nrows` coefficients (otherwise the raw
+/// entry point reports the shape error).
+fn wide_terms<'a, F: CudaField>(terms: &[(&[F::Elem], DeviceSlice<'a>)], nrows: usize)
+                                -> Option<(Plan<F>, Vec<DeviceSlice<'a>>)> {
+    if !F::WIDE || terms.is_empty() || terms.iter().any(|(c, _)| c.len() != nrows) {
+        return None;
+    }
+    let vals: Vec<F::Elem> = terms.iter().flat_map(|(c, _)| c.iter().copied()).collect();
+    Some((Plan::matrix(terms.len(), nrows, &vals), terms.iter().map(|(_, s)| *s).collect()))
+}
+
 fn terms<F: CudaField>(terms: &[(&[F::Elem], DeviceSlice<'_>)]) -> (Vec<Vec<u32>>, Vec<sys::fgfc_term>) {
     let coeffs: Vec<Vec<u32>> = terms.iter().map(|(c, _)| raw::<F>(c)).collect();
     let raws = terms
@@ -379,6 +436,9 @@ fn terms<F: CudaField>(terms: &[(&[F::Elem], DeviceSlice<'_>)]) -> (Vec<Vec<u32>
 #[track_caller]
 pub fn mul_add_matrix<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_len: usize, nrows: usize,
                                     terms_: &[(&[F::Elem], DeviceSlice<'_>)]) {
+    if let Some((plan, srcs)) = wide_terms::<F>(terms_, nrows) {
+        return mul_add_matrix_with(rows, row_len, nrows, &plan, &srcs);
+    }
     let (_keep, t) = terms::<F>(terms_);
     check(unsafe {
         sys::fgfc_mul_add_matrix(F::ID, rows.as_mut_ptr(), rows.len(), row_len, nrows, t.as_ptr(), t.len(), stream())
@@ -400,6 +460,9 @@ pub fn mul_add_matrix_with<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_len:
 #[track_caller]
 pub fn dot_product_matrix<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_len: usize, nrows: usize,
                                         terms_: &[(&[F::Elem], DeviceSlice<'_>)]) {
+    if let Some((plan, srcs)) = wide_terms::<F>(terms_, nrows) {
+        return dot_product_matrix_with(rows, row_len, nrows, &plan, &srcs);
+    }
     let (_keep, t) = terms::<F>(terms_);
     check(unsafe {
         sys::fgfc_dot_product_matrix(F::ID, rows.as_mut_ptr(), rows.len(), row_len, nrows, t.as_ptr(), t.len(), stream())
@@ -421,6 +484,9 @@ pub fn dot_product_matrix_with<F: CudaField>(rows: &mut DeviceSliceMut<'_>, row_
 #[track_caller]
 pub fn mul_add_matrix_scattered<F: CudaField>(dst: &mut DeviceSliceMut<'_>, row_len: usize, row_starts: &[usize],
                                               terms_: &[(&[F::Elem], DeviceSlice<'_>)]) {
+    if let Some((plan, srcs)) = wide_terms::<F>(terms_, row_starts.len()) {
+        return mul_add_matrix_scattered_with(dst, row_len, row_starts, &plan, &srcs);
+    }
     let (_keep, t) = terms::<F>(terms_);
     check(unsafe {
         sys::fgfc_mul_add_matrix_scattered(F::ID, dst.as_mut_ptr(), dst.len(), row_len, row_starts.as_ptr(),

@@ -16,6 +16,8 @@ pub const FGFC_GF32: fgfc_field = 3;
 pub const FGFC_FP8: fgfc_field = 4;
 pub const FGFC_FP16: fgfc_field = 5;
 pub const FGFC_FP32: fgfc_field = 6;
+pub const FGFC_GF64: fgfc_field = 7;
+pub const FGFC_FP64: fgfc_field = 8;
 
 pub const FGFC_OK: fgfc_status = 0;
 pub const FGFC_ERR_WIDTH: fgfc_status = 1;
@@ -173,12 +175,17 @@ extern "C" {
     pub fn fgfc_plan_create(field: fgfc_field, rows: usize, cols: usize, coeffs: *const u32,
                             out: *mut *mut fgfc_plan) -> fgfc_status;
     pub fn fgfc_coeff_create(field: fgfc_field, coeff: u32, out: *mut *mut fgfc_plan) -> fgfc_status;
+    pub fn fgfc_plan_create_u64(field: fgfc_field, rows: usize, cols: usize, coeffs: *const u64,
+                                out: *mut *mut fgfc_plan) -> fgfc_status;
+    pub fn fgfc_coeff_create_u64(field: fgfc_field, coeff: u64, out: *mut *mut fgfc_plan) -> fgfc_status;
     pub fn fgfc_plan_destroy(plan: *mut fgfc_plan);
     pub fn fgfc_plan_dimensions(plan: *const fgfc_plan, rows: *mut usize, cols: *mut usize) -> fgfc_status;
     pub fn fgfc_plan_len(plan: *const fgfc_plan) -> usize;
     pub fn fgfc_plan_field(plan: *const fgfc_plan) -> fgfc_field;
     pub fn fgfc_plan_values(plan: *const fgfc_plan, out: *mut u32) -> fgfc_status;
     pub fn fgfc_plan_get_at(plan: *const fgfc_plan, row: usize, col: usize, out: *mut u32) -> fgfc_status;
+    pub fn fgfc_plan_values_u64(plan: *const fgfc_plan, out: *mut u64) -> fgfc_status;
+    pub fn fgfc_plan_get_at_u64(plan: *const fgfc_plan, row: usize, col: usize, out: *mut u64) -> fgfc_status;
 
     pub fn fgfc_add_assign(field: fgfc_field, dst: *mut u8, dst_len: usize, src: *const u8, src_len: usize,
                            stream: fgfc_stream) -> fgfc_status;

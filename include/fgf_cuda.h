@@ -50,7 +50,13 @@ typedef enum fgfc_field {
      top generator; elements lo + hi*X, little-endian. */
   FGFC_FP8 = 4,  /* Fan-Paar GF(2^8), 1 byte  (fan_paar::fp8, FanPaar8) */
   FGFC_FP16 = 5, /* Fan-Paar GF(2^16), 2 bytes (fan_paar::fp16, FanPaar16) */
-  FGFC_FP32 = 6  /* Fan-Paar GF(2^32), 4 bytes (fan_paar::fp32, FanPaar32) */
+  FGFC_FP32 = 6, /* Fan-Paar GF(2^32), 4 bytes (fan_paar::fp32, FanPaar32) */
+  /* 8-byte fields. Their coefficients are 64-bit: make plans with
+     fgfc_plan_create_u64 / fgfc_coeff_create_u64 and use the _with entry
+     points; a raw entry point's uint32_t coefficient is the element whose
+     high 32 bits are zero. */
+  FGFC_GF64 = 7, /* GF(2^32)[w]/(w^2+w+0x20000000), 8 bytes LE (src/field/gf64.rs:1-11) */
+  FGFC_FP64 = 8  /* Fan-Paar GF(2^64), 8 bytes (fan_paar::fp64, FanPaar64) */
 } fgfc_field;
 
 typedef enum fgfc_status {
@@ -109,6 +115,11 @@ fgfc_status fgfc_plan_create(fgfc_field field, size_t rows, size_t cols, const u
                              fgfc_plan **out);
 /* Coeff::new(coeff) (ops.rs:61-65): a 1x1 plan. */
 fgfc_status fgfc_coeff_create(fgfc_field field, uint32_t coeff, fgfc_plan **out);
+/* The same with 64-bit coefficients, for every field (the 8-byte fields need
+ * them; values are reduced to the field's width as above). */
+fgfc_status fgfc_plan_create_u64(fgfc_field field, size_t rows, size_t cols, const uint64_t *coeffs,
+                                 fgfc_plan **out);
+fgfc_status fgfc_coeff_create_u64(fgfc_field field, uint64_t coeff, fgfc_plan **out);
 void fgfc_plan_destroy(fgfc_plan *plan);
 /* Plan::dimensions (ops.rs:231-233), Plan::len (ops.rs:217-219). */
 fgfc_status fgfc_plan_dimensions(const fgfc_plan *plan, size_t *rows, size_t *cols);
@@ -118,6 +129,10 @@ fgfc_field fgfc_plan_field(const fgfc_plan *plan);
 fgfc_status fgfc_plan_values(const fgfc_plan *plan, uint32_t *out);
 /* Plan::get_at(row, col).value() (ops.rs:247-251); ERR_ARG when out of bounds. */
 fgfc_status fgfc_plan_get_at(const fgfc_plan *plan, size_t row, size_t col, uint32_t *out);
+/* Plan::values / Plan::get_at with 64-bit values (the 32-bit forms return
+ * the low halves of an 8-byte field's coefficients). */
+fgfc_status fgfc_plan_values_u64(const fgfc_plan *plan, uint64_t *out);
+fgfc_status fgfc_plan_get_at_u64(const fgfc_plan *plan, size_t row, size_t col, uint64_t *out);
 
 /* ---------------------------------------------------------------- single row */
 

@@ -58,7 +58,11 @@ def _u32(v) -> np.ndarray:
 
 
 def _u64(v) -> np.ndarray:
-    return np.ascontiguousarray(np.asarray([int(x) for x in np.asarray(v).reshape(-1)], dtype=np.uint64))
+    # Python ints are converted one by one: np.asarray of a list that mixes
+    # values below and at or above 2^63 would go through float64 and round.
+    if isinstance(v, np.ndarray):
+        return np.ascontiguousarray(v.reshape(-1).astype(np.uint64))
+    return np.ascontiguousarray(np.array([int(x) & 0xFFFFFFFFFFFFFFFF for x in v], dtype=np.uint64))
 
 
 def _ptrs(srcs) -> C.Array:

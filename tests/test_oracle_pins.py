@@ -293,3 +293,29 @@ def test_fan_paar_64_vectors():
 
 def test_wide_field_names():
     assert fields.Gf64.NAME == WIDE["names"]["gf64"] and fields.FanPaar64.NAME == WIDE["names"]["fp64"]
+
+
+@pytest.mark.parametrize("fid", [orc.GF64, orc.FP64])
+def test_wide_oracle_ops_agree_with_the_scalar_product(fid):
+    """The oracle's vector ops with 64-bit coefficients (including values at
+    and above 2^63) equal the scalar product applied element by element."""
+    ln, m = 8 * 40, 3
+    c = [0x8000000100000003, 5, 0xFFFFFFFFFFFFFFFF]
+    src = orc.noise(ln, 1)
+    rows = orc.noise(m * ln, 2)
+    want = rows.copy().view("<u8")
+    x = src.view("<u8")
+    for j in range(m):
+        for i in range(ln // 8):
+            want[j * (ln // 8) + i] ^= np.uint64(orc.mul64(fid, c[j], int(x[i])))
+    got = rows.copy()
+    orc.mul_add_scatter(fid, got, ln, c, src)
+    assert np.array_equal(got.view("<u8"), want)
+    srcs = [orc.noise(ln, 10 + t) for t in range(m)]
+    got = np.zeros(ln, np.uint8)
+    orc.dot_product(fid, got, c, srcs)
+    want = np.zeros(ln // 8, np.uint64)
+    for t in range(m):
+        for i, v in enumerate(srcs[t].view("<u8")):
+            want[i] ^= np.uint64(orc.mul64(fid, c[t], int(v)))
+    assert np.array_equal(got.view("<u8"), want)
