@@ -781,6 +781,41 @@ def leg_tower_and_large_km(dev):
     return out
 
 
+def leg_wide_fields(dev, L: int = 16 * MIB):
+    """The 8-byte fields (GF(2^64), Fan-Paar GF(2^64)): RS(10,4) encode with
+    dot_product_matrix_with on 16 MiB shards, uniformly random 64-bit
+    coefficients, on the 8-byte table kernel; checked against the oracle on
+    column windows."""
+    import torch
+
+    from fgf_b200 import ops
+    from fgf_b200.fields import FanPaar64, Gf64
+
+    peak = hbm_peak()[0]
+    out = {}
+    stream = torch.cuda.current_stream(dev)
+    k, m = 10, 4
+    for name, field in (("gf64_rs10_4_16MiB", Gf64), ("fp64_rs10_4_16MiB", FanPaar64)):
+        rng = np.random.default_rng(0x64 + field.ID)
+        g = torch.Generator(device=dev)
+        g.manual_seed(0x64 + field.ID)
+        vals = [int(x) for x in rng.integers(1, 1 << 64, size=k * m, dtype=np.uint64)]
+        plan = ops.Plan.matrix(field, k, m, vals)
+        buf = torch.randint(0, 256, ((k + m) * L,), dtype=torch.uint8, device=dev, generator=g)
+        srcs = [buf[t * L:(t + 1) * L] for t in range(k)]
+        rows = buf[k * L:]
+        rows.fill_(0xA5)
+        ops.dot_product_matrix_with(rows, L, m, plan, srcs, stream)
+        torch.cuda.synchronize()
+        ok = oracle_matrix_windows(field.ID, srcs, None, [rows[j * L:(j + 1) * L] for j in range(m)], vals, True, rng)
+        ms = event_ms(lambda: ops.dot_product_matrix_with(rows, L, m, plan, srcs, stream), 10, stream)
+        out[name] = {"ms": round(ms, 4), "source_GB/s": round(k * L / ms / 1e6, 1),
+                     "hbm_frac": round((k + m) * L / ms / 1e6 / peak, 4), "oracle_windows": "passed" if ok else "FAILED"}
+        del buf
+        torch.cuda.empty_cache()
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 
 def pcie_duplex(dev, nbytes: int = 1 << 30) -> dict:
@@ -1089,6 +1124,7 @@ def run_ours(args):
         legs["config1_single_row_256MiB"] = leg_single_row_ops(dev)
         torch.cuda.empty_cache()
         legs["config2_tower_large_km"] = leg_tower_and_large_km(dev)
+        legs["fields_64bit_rs10_4"] = leg_wide_fields(dev)
         torch.cuda.empty_cache()
         extra["legs"] = legs
         compact["c0_us_per_call"] = legs["config0_single_stripe_64KiB"]["us_per_call"]
@@ -1100,6 +1136,8 @@ def run_ours(args):
         for k_, v_ in legs["config2_tower_large_km"].items():
             compact[f"c2_{k_}_source_GBps"] = v_[v_["chosen"]]["source_GB/s"]
             compact[f"c2_{k_}_kernel"] = v_["chosen"]
+        for k_, v_ in legs["fields_64bit_rs10_4"].items():
+            compact[f"{k_}_source_GBps"] = v_["source_GB/s"]
     if world == 1 and not args.no_uneven:
         u = uneven_batch(dev, args.uneven_stripes, 5)
         extra["uneven_batch"] = u
@@ -1151,6 +1189,7 @@ CASES = {
     # name: (field name, k, m) for dot_product_matrix_with, or an op name
     "c2_gf16": ("Gf16", 32, 8), "c2_gf32": ("Gf32", 16, 4), "c2_gf8b": ("Gf8B", 64, 16),
     "rs104_encode": ("Gf8D", 10, 4), "gf16_rs8_2": ("Gf16", 8, 2),
+    "gf64_rs104": ("Gf64", 10, 4), "fp64_rs104": ("FanPaar64", 10, 4),
     "axpy": "mul_add", "scatter": "mul_add_scatter", "gather": "mul_add_gather",
     "xor": "add_assign", "elementwise": "mul_elementwise", "uneven": "uneven",
 }
@@ -1188,7 +1227,7 @@ def run_case(args):
         torch.cuda.synchronize()
         ok = oracle_matrix_windows(field.ID, srcs, None, [rows[j * n:(j + 1) * n] for j in range(m)], vals, True, rng)
         alg, src_b = (k + m) * n, k * n
-        kernel = tune.chosen(field, k, m, n)
+        kernel = "wide" if field.BYTES == 8 else tune.chosen(field, k, m, n)
     elif spec == "uneven":
         res = uneven_batch(dev, max(16, int(args.case_mib)), max(1, args.steps))
         print(json.dumps({"case": args.case, **res}))

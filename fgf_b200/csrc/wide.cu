@@ -83,8 +83,10 @@ __global__ void __launch_bounds__(kWideThreads) wide_kernel(const __grid_constan
     uint32_t acc[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) acc[g] = 0;
+    uint64_t next = load8(a.src[0] + 8 * e);
     for (uint32_t t = 0; t < a.k; ++t) {
-      const uint64_t x = load8(a.src[t] + 8 * e);
+      const uint64_t x = next;  // the next source's element is in flight during this one's lookups
+      if (t + 1 < a.k) next = load8(a.src[t + 1] + 8 * e);
       const uint32_t* tt = tab + t * 8u * G * 32u;
 #pragma unroll
       for (int p = 0; p < 8; ++p) {
@@ -159,8 +161,13 @@ cudaError_t wide_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t
       const size_t smem = kk * per_src_words * 4;
       cudaError_t e = ensure_smem_attr(reinterpret_cast<const void*>(fn), static_cast<int>(smem));
       if (e != cudaSuccess) return e;
+      // One wave of resident CTAs: each loads its tables into shared memory once.
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWideThreads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
       const uint64_t want = (nelem + kWideThreads - 1) / kWideThreads;
-      const unsigned grid = static_cast<unsigned>(std::min<uint64_t>(want, static_cast<uint64_t>(sm_count()) * 4));
+      const unsigned grid =
+          static_cast<unsigned>(std::min<uint64_t>(want, static_cast<uint64_t>(sm_count()) * static_cast<uint64_t>(per_sm)));
       {
         std::lock_guard<std::mutex> lk(g_wide_mu);
         fn<<<grid, kWideThreads, smem, stream>>>(a);
