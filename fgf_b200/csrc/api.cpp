@@ -251,26 +251,33 @@ fgfc_status upload_plan_tables(fgfc_plan* p) {
   const int E = field_bytes(p->field);
   const size_t len = p->values.size();
   // 4-byte output groups covering n rows of E-byte elements
-  const auto groups = [E](size_t n) { return (n * E + 3) / 4; };
+  // Per source: E input bytes x (groups) slots of compact tables; the
+  // 8-byte fields keep their half-product tables instead (build_wide_tables:
+  // 12 slots per source and row, "groups" counting rows).
+  const bool wide = E == 8;
+  const auto groups = [E, wide](size_t n) { return wide ? n : (n * E + 3) / 4; };
+  const size_t slots_per_src = wide ? kWideSlotsPerSrcRow : static_cast<size_t>(E);
+  const auto build = [&](const uint64_t* c, size_t m, size_t k, size_t G, uint32_t* out) {
+    if (wide)
+      build_wide_tables(p->field, c, m, 0, k, 0, G, out);
+    else
+      build_compact_tables(p->field, c, m, 0, k, 0, G, out);
+  };
   // matrix orientation: rows = sources, cols = destination rows
   p->mat_groups = groups(p->cols);
-  const size_t n_mat = p->rows * E * p->mat_groups * kCompactWords;
+  const size_t n_mat = p->rows * slots_per_src * p->mat_groups * kCompactWords;
   p->scat_groups = groups(len);
-  const size_t n_scat = E * p->scat_groups * kCompactWords;
+  const size_t n_scat = slots_per_src * p->scat_groups * kCompactWords;
   p->gath_groups = groups(1);
-  const size_t n_gath = len * E * p->gath_groups * kCompactWords;
+  const size_t n_gath = len * slots_per_src * p->gath_groups * kCompactWords;
   std::vector<uint32_t> host(n_mat + n_scat + n_gath + 1, 0);
   p->off_mat = 0;
   p->off_scat = n_mat;
   p->off_gath = n_mat + n_scat;
-  if (n_mat) build_compact_tables(p->field, p->values.data(), p->cols, 0, p->rows, 0, p->mat_groups,
-                                  host.data() + p->off_mat);
-  if (n_scat) build_compact_tables(p->field, p->values.data(), len, 0, 1, 0, p->scat_groups,
-                                   host.data() + p->off_scat);
-  if (n_gath) {
-    // gather orientation: source i has the single coefficient values[i]
-    build_compact_tables(p->field, p->values.data(), 1, 0, len, 0, p->gath_groups, host.data() + p->off_gath);
-  }
+  if (n_mat) build(p->values.data(), p->cols, p->rows, p->mat_groups, host.data() + p->off_mat);
+  if (n_scat) build(p->values.data(), len, 1, p->scat_groups, host.data() + p->off_scat);
+  // gather orientation: source i has the single coefficient values[i]
+  if (n_gath) build(p->values.data(), 1, len, p->gath_groups, host.data() + p->off_gath);
   if (n_mat && gf2mma_shape_ok(p->field, p->rows, p->cols)) {
     p->bits_mat.resize(kGf2BitWords);
     gf2mma_bits(p->field, p->values.data(), p->rows, p->cols, p->bits_mat.data());

@@ -51,6 +51,21 @@ struct MatrixLaunch {
 void build_compact_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k,
                           size_t g0, size_t G, uint32_t* out);
 
+// The 8-byte fields multiply a constant c = c0 + c1 w by x = x0 + x1 w
+// (halves over the 4-byte base field: Gf32 for GF(2^64), FP32 for Fan-Paar
+// GF(2^64)) as three half-products A = c0 x0, B = c1 x1, C = (c0 + c1)(x0 + x1)
+// and a fix-up of the sums (Karatsuba): GF(2^64) gives lo = A + beta B,
+// hi = A + C; Fan-Paar gives lo = A + B, hi = A + C + (1 + alpha) B. Tables
+// for sources [t0, t0+k) and rows [j0, j0+M), layout
+// [((t * 3 + P) * 4 + p) * M + j][32]: product P (A, B, C), input byte p of
+// the 4-byte half, 16 words for its low nibble and 16 for its high nibble.
+constexpr size_t kWideSlotsPerSrcRow = 12;
+void build_wide_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k, size_t j0, size_t M,
+                       uint32_t* out);
+// The fix-up map of an 8-byte field as [4 input bytes][32] nibble tables:
+// v -> beta v (GF(2^64)) or v -> (1 + alpha) v (Fan-Paar GF(2^64)).
+void build_wide_fixup(int field, uint32_t* out /* [128] */);
+
 // Kernel entry (kernels.cu). `groups` = G for this launch; `overwrite`
 // selects dot-product (overwrite) or mul_add (accumulate) semantics.
 // `byte_tables`: run the byte-table kernel (Gf8, one group, <= 14 sources)
@@ -140,6 +155,9 @@ void lower_matrix_job(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, 
 // host values (term-major k x m, tables built into the launch parameters) or
 // as a plan's device tables in the compact layout with `gstride` groups per
 // (source, byte plane).
+// Matrix ops of the 8-byte fields (wide.cu): dev_tables in the
+// build_wide_tables layout with `gstride` rows, or nullptr (tables built
+// per launch from host_coeffs).
 cudaError_t wide_launch(int field, const uint8_t* const* srcs, size_t k, uint8_t* const* rows, size_t m,
                         const uint64_t* host_coeffs, const uint32_t* dev_tables, size_t gstride, size_t len,
                         bool overwrite, cudaStream_t stream);

@@ -56,4 +56,53 @@ void build_compact_tables(int field, const uint64_t* coeffs, size_t m, size_t t0
   }
 }
 
+namespace {
+
+// c * x over the 4-byte base field of an 8-byte field.
+uint32_t wide_half_mul(int field, uint32_t c, uint32_t x) {
+  return field == kGf64 ? gf32_mul(c, x) : static_cast<uint32_t>(fp_mul(c, x, 32));
+}
+
+// Nibble tables of a GF(2)-linear map on 32-bit words, given the images of
+// its 32 input bits: table p (input byte p) at out + p * 32.
+void linear_tables(const uint32_t img[32], uint32_t* out, size_t stride_slots) {
+  for (int p = 0; p < 4; ++p) {
+    uint32_t* slot = out + p * stride_slots * kCompactWords;
+    for (int half = 0; half < 2; ++half)
+      for (int n = 0; n < 16; ++n) {
+        uint32_t v = 0;
+        for (int b = 0; b < 4; ++b)
+          if ((n >> b) & 1) v ^= img[8 * p + 4 * half + b];
+        slot[half * 16 + n] = v;
+      }
+  }
+}
+
+}  // namespace
+
+void build_wide_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k, size_t j0, size_t M,
+                       uint32_t* out) {
+  for (size_t tt = 0; tt < k; ++tt)
+    for (size_t j = 0; j < M; ++j) {
+      const uint64_t c = coeffs[(t0 + tt) * m + j0 + j];
+      const uint32_t c0 = static_cast<uint32_t>(c), c1 = static_cast<uint32_t>(c >> 32);
+      const uint32_t cp[3] = {c0, c1, c0 ^ c1};
+      for (int P = 0; P < 3; ++P) {
+        uint32_t img[32];
+        for (int i = 0; i < 32; ++i) img[i] = wide_half_mul(field, cp[P], 1u << i);
+        // slot of (tt, P, p = 0, j); input byte p is M slots further on
+        linear_tables(img, out + ((tt * 3 + P) * 4 * M + j) * kCompactWords, M);
+      }
+    }
+}
+
+void build_wide_fixup(int field, uint32_t* out) {
+  uint32_t img[32];
+  for (int i = 0; i < 32; ++i) {
+    const uint32_t v = 1u << i;
+    img[i] = field == kGf64 ? gf32_mul(0x20000000u, v) : v ^ static_cast<uint32_t>(fp_mul_alpha(v, 32));
+  }
+  linear_tables(img, out, 1);
+}
+
 }  // namespace fgfc
