@@ -1178,7 +1178,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded uniform random bytes; seeded erasure patterns)",
             "config": config(args, L), "roofline": roof, "cpu_baseline": cpu, "cpu_baseline_1core": cpu1,
-            "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "parity_check": "passed", **compact, **extra}
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "parity_check": "passed",
+            "value_GiBps": round(value * 1e9 / 2 ** 30, 2), **compact, **extra}
     print(json.dumps(line))
     return 0
 
