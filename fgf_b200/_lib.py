@@ -201,6 +201,10 @@ _SIGS = {
     "fgfc_tune_choice": (C.c_int, [C.c_int, c_size, c_size, c_size]),
     "fgfc_tune_usable": (C.c_int, [C.c_int, C.c_int, c_size, c_size]),
     "fgfc_tune_shape": (c_status, [C.c_int, c_size, c_size, c_size, C.POINTER(C.c_int)]),
+    "fgfc_tune_set_tile": (c_status, [c_size, c_size, C.c_uint]),
+    "fgfc_tune_tile": (C.c_uint, [c_size, c_size]),
+    "fgfc_tune_batch_tiles": (c_status, [C.c_void_p, C.POINTER(MatrixJob), c_size, c_stream,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "fgfc_tune_save": (c_status, [C.c_char_p]),
     "fgfc_tune_load": (c_status, [C.c_char_p]),
     "fgfc_tune_clear": (None, []),

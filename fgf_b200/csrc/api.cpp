@@ -1144,6 +1144,64 @@ fgfc_status fgfc_batch_run(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_
   return e == cudaSuccess ? ok() : cuda_fail(e, "batch");
 }
 
+// Tile shapes measured on one submission. A timing is the minimum over 3
+// reps of one submission, each enqueued right behind an untimed one, so the
+// host's lowering of the timed submission overlaps the device's work and
+// the events bracket device time only.
+fgfc_status fgfc_tune_batch_tiles(fgfc_batch* batch, const fgfc_matrix_job* jobs, size_t njobs, fgfc_stream stream,
+                                  double* us_before, double* us_after) {
+  if (!batch || (njobs && !jobs)) return fail(FGFC_ERR_ARG, "tune_batch_tiles: null argument");
+  fgfc_status st = fgfc_batch_run(batch, jobs, njobs, stream);  // validates; records the classes
+  if (st != FGFC_OK) return st;
+  const std::vector<std::pair<int, int>> classes = batch_state_classes(batch->state);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  double best_total = 0;
+  const auto time_us = [&](double* out) -> fgfc_status {
+    double best = 1e300;
+    for (int rep = 0; rep < 3; ++rep) {
+      fgfc_status s2 = fgfc_batch_run(batch, jobs, njobs, stream);
+      if (s2 == FGFC_OK && cudaEventRecord(e0, stream) != cudaSuccess) s2 = fail(FGFC_ERR_CUDA, "tune_batch_tiles: event");
+      if (s2 == FGFC_OK) s2 = fgfc_batch_run(batch, jobs, njobs, stream);
+      if (s2 == FGFC_OK && (cudaEventRecord(e1, stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+        s2 = fail(FGFC_ERR_CUDA, "tune_batch_tiles: event");
+      if (s2 != FGFC_OK) return s2;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best = std::min(best, 1e3 * static_cast<double>(ms));
+    }
+    *out = best;
+    return FGFC_OK;
+  };
+  if (e != cudaSuccess) st = cuda_fail(e, "tune_batch_tiles");
+  if (st == FGFC_OK) st = time_us(&best_total);
+  if (st == FGFC_OK && us_before) *us_before = best_total;
+  // one class at a time, the others at their current tiles
+  for (size_t ci = 0; ci < classes.size() && st == FGFC_OK; ++ci) {
+    const int E = classes[ci].first, G = classes[ci].second;
+    const int start = tile_cols(E, G);
+    int best_cols = start;
+    for (int cols : {1, 2, 4, 8, 16}) {
+      if (cols == start) continue;
+      set_tile_cols(E, G, cols, 0.0);
+      double us = 0;
+      st = time_us(&us);
+      if (st != FGFC_OK) break;
+      if (us < best_total * 0.98) {  // a clear win only
+        best_total = us;
+        best_cols = cols;
+      }
+    }
+    set_tile_cols(E, G, best_cols, best_total);
+  }
+  if (st == FGFC_OK) st = time_us(&best_total);
+  if (st == FGFC_OK && us_after) *us_after = best_total;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return st == FGFC_OK ? ok() : st;
+}
+
 fgfc_status fgfc_run_jobs_serial(const fgfc_matrix_job* jobs, size_t njobs, fgfc_stream stream) {
   if (njobs && !jobs) return fail(FGFC_ERR_ARG, "batch: null argument");
   for (size_t i = 0; i < njobs; ++i) {

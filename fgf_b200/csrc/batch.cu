@@ -681,7 +681,8 @@ struct BatchState {
   cudaEvent_t fork = nullptr, join[kSideStreams] = {};
   size_t last_launches = 0, last_items = 0;
   int last_replayed = 0;
-  std::mutex mu;
+  std::vector<std::pair<int, int>> last_classes;  // nibble (E, G) classes of the last submission
+  mutable std::mutex mu;
 };
 
 static cudaError_t ensure_slot(BatchSlot& s, size_t bytes) {
@@ -732,6 +733,15 @@ void batch_state_destroy(void* p) {
 
 void batch_state_graphs(void* p, bool on) { static_cast<BatchState*>(p)->graphs = on; }
 
+std::vector<std::pair<int, int>> batch_state_classes(const void* p) {
+  const BatchState* b = static_cast<const BatchState*>(p);
+  std::lock_guard<std::mutex> lk(b->mu);
+  std::vector<std::pair<int, int>> v = b->last_classes;
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  return v;
+}
+
 void batch_state_stats(const void* p, size_t* launches, size_t* items, int* replayed) {
   const BatchState* b = static_cast<const BatchState*>(p);
   if (launches) *launches = b->last_launches;
@@ -747,6 +757,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
   std::lock_guard<std::mutex> lk(b->mu);
   b->last_launches = b->last_items = 0;
   b->last_replayed = 0;
+  b->last_classes.clear();
   if (jobs.empty() && tc.empty()) return cudaSuccess;
 
   // ---- device descriptors, pointer array, classes (sub-jobs in plan order)
@@ -794,15 +805,18 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
     for (uint32_t i : c.jobs)
       c.uniform = c.uniform && jobs[i].tables == jobs[c.jobs[0]].tables && jobs[i].g0 == jobs[c.jobs[0]].g0;
     if (c.uniform) continue;
-    // Columns per item: up to 8 per thread, fewer when the class is too
-    // small to give every SM a few items (a small class runs beside the
-    // others on its own stream, see enqueue).
+    // Columns per item: the class's tile (tune.cpp: tile_cols; 8 per
+    // thread built in) for nibble classes, 8 per thread for byte-table
+    // classes, fewer when the class is too small to give every SM a few
+    // items (a small class runs beside the others on its own stream, see
+    // enqueue).
     const uint64_t threads = c.K ? kFastThreads : kThreads;
+    const uint64_t tile = c.K ? kFastVecPerItem : threads * static_cast<uint64_t>(tile_cols(c.E, c.G));
+    if (!c.K) b->last_classes.emplace_back(c.E, c.G);
     uint64_t total = 0;
     for (uint32_t i : c.jobs) total += jobs[i].nvec;
     const uint64_t want = (total + 4 * static_cast<uint64_t>(sm_count()) - 1) / (4 * static_cast<uint64_t>(sm_count()));
-    const uint64_t per_vec = std::min<uint64_t>(c.K ? kFastVecPerItem : kVecPerItem,
-                                                std::max<uint64_t>(threads, (want + threads - 1) / threads * threads));
+    const uint64_t per_vec = std::min<uint64_t>(tile, std::max<uint64_t>(threads, (want + threads - 1) / threads * threads));
     const uint64_t per_grp = c.K ? kFastGroupsPerItem : kGroupsPerItem;
     for (uint32_t i : c.jobs) {
       const LoweredJob& L = jobs[i];

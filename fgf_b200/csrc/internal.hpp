@@ -86,6 +86,12 @@ int sm_count();
 constexpr size_t kFastMaxSources = 14;  // byte-table kernels: sources per launch
 bool kernel_usable(int kernel, int field, size_t k, size_t m);
 int choose_kernel(int field, size_t k, size_t m, size_t len);
+// Tile shape of the batched nibble work lists (tune.cpp): element-vector
+// columns per thread per work item for the class of element width E and G
+// table groups; set_tile_cols(E, G, 0) restores the built-in value.
+constexpr int kTileColsDefault = 8;
+int tile_cols(int E, int G);
+void set_tile_cols(int E, int G, int cols, double us);
 // Shapes the bit-sliced tensor-core contraction covers in one launch
 // (gf2mma.cu): at most 512 input bits and 128 output bits per element column.
 bool gf2mma_shape_ok(int field, size_t k, size_t m);
@@ -142,6 +148,9 @@ struct Gf2Job {
 void* batch_state_create();
 void batch_state_destroy(void* state);
 void batch_state_graphs(void* state, bool on);
+// The nibble work-list classes (element width, table groups) of the state's
+// last submission.
+std::vector<std::pair<int, int>> batch_state_classes(const void* state);
 void batch_state_stats(const void* state, size_t* launches, size_t* items, int* replayed);
 cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const std::vector<Gf2Job>& tc,
                       cudaStream_t stream);

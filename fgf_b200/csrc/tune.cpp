@@ -47,6 +47,27 @@ struct TuneVal {
 
 std::map<TuneKey, TuneVal> g_table;
 
+// Tile shape of the batched nibble work lists: element-vector columns per
+// thread per work item, by (element width, table groups); 0 = built-in.
+// FGFC_TILE_COLS=n in the environment (read once) overrides every class.
+struct TileVal {
+  int cols;
+  double us;
+};
+std::map<std::pair<int, int>, TileVal> g_tiles;
+int g_tile_env = -1;  // -1: environment not read yet, 0: unset
+
+bool tile_ok(int cols) { return cols == 1 || cols == 2 || cols == 4 || cols == 8 || cols == 16; }
+
+int tile_env_locked() {
+  if (g_tile_env < 0) {
+    const char* v = std::getenv("FGFC_TILE_COLS");
+    const int n = v ? std::atoi(v) : 0;
+    g_tile_env = tile_ok(n) ? n : 0;
+  }
+  return g_tile_env;
+}
+
 uint32_t len_bucket(size_t len) {  // floor(log2(len)), 0 for 0
   uint32_t b = 0;
   while (len > 1) {
@@ -113,6 +134,21 @@ int choose_kernel(int field, size_t k, size_t m, size_t len) {
   const auto it = g_table.find(TuneKey{field, static_cast<uint32_t>(k), static_cast<uint32_t>(m), len_bucket(len)});
   if (it != g_table.end() && kernel_usable(it->second.kernel, field, k, m)) return it->second.kernel;
   return builtin_choice(field, k, m, len);
+}
+
+int tile_cols(int E, int G) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (const int env = tile_env_locked()) return env;
+  const auto it = g_tiles.find({E, G});
+  return it != g_tiles.end() ? it->second.cols : kTileColsDefault;
+}
+
+void set_tile_cols(int E, int G, int cols, double us) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (cols == 0)
+    g_tiles.erase({E, G});
+  else
+    g_tiles[{E, G}] = TileVal{cols, us};
 }
 
 }  // namespace fgfc
@@ -217,6 +253,18 @@ fgfc_status fgfc_tune_shape(fgfc_field field, size_t nsrcs, size_t nrows, size_t
   return clear_error();
 }
 
+fgfc_status fgfc_tune_set_tile(size_t elem_bytes, size_t groups, unsigned cols) {
+  if ((elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4) || groups < 1 || groups > 4 ||
+      (cols != 0 && !tile_ok(static_cast<int>(cols))))
+    return set_error(FGFC_ERR_ARG, "tune_set_tile: invalid class or tile (columns 1, 2, 4, 8, 16 or 0)");
+  set_tile_cols(static_cast<int>(elem_bytes), static_cast<int>(groups), static_cast<int>(cols), 0.0);
+  return clear_error();
+}
+
+unsigned fgfc_tune_tile(size_t elem_bytes, size_t groups) {
+  return static_cast<unsigned>(tile_cols(static_cast<int>(elem_bytes), static_cast<int>(groups)));
+}
+
 fgfc_status fgfc_tune_save(const char* path) {
   if (!path) return set_error(FGFC_ERR_ARG, "tune_save: null path");
   std::lock_guard<std::mutex> lk(g_mu);
@@ -228,6 +276,13 @@ fgfc_status fgfc_tune_save(const char* path) {
     std::fprintf(f, "%s\n  {\"field\": %d, \"k\": %u, \"m\": %u, \"len_log2\": %u, \"kernel\": \"%s\", \"us\": %.3f}",
                  first ? "" : ",", kv.first.field, kv.first.k, kv.first.m, kv.first.lb, kernel_name(kv.second.kernel),
                  kv.second.us);
+    first = false;
+  }
+  std::fprintf(f, "\n], \"tiles\": [");
+  first = true;
+  for (const auto& kv : g_tiles) {
+    std::fprintf(f, "%s\n  {\"elem_bytes\": %d, \"groups\": %d, \"cols\": %d, \"us\": %.3f}", first ? "" : ",",
+                 kv.first.first, kv.first.second, kv.second.cols, kv.second.us);
     first = false;
   }
   std::fprintf(f, "\n]}\n");
@@ -242,6 +297,7 @@ fgfc_status fgfc_tune_load(const char* path) {
   if (!f) return set_error(FGFC_ERR_ARG, "tune_load: cannot open file");
   char line[512];
   std::map<TuneKey, TuneVal> got;
+  std::map<std::pair<int, int>, TileVal> tiles;
   while (std::fgets(line, sizeof line, f)) {
     int field;
     unsigned k, m, lb;
@@ -249,6 +305,11 @@ fgfc_status fgfc_tune_load(const char* path) {
     double us;
     const char* p = std::strchr(line, '{');
     if (!p || std::strstr(line, "\"version\"")) continue;
+    int te, tg, tc;
+    if (std::sscanf(p, " {\"elem_bytes\": %d, \"groups\": %d, \"cols\": %d, \"us\": %lf", &te, &tg, &tc, &us) == 4) {
+      if ((te == 1 || te == 2 || te == 4) && tg >= 1 && tg <= 4 && tile_ok(tc)) tiles[{te, tg}] = TileVal{tc, us};
+      continue;
+    }
     if (std::sscanf(p, " {\"field\": %d, \"k\": %u, \"m\": %u, \"len_log2\": %u, \"kernel\": \"%31[a-z0-9]\", \"us\": %lf",
                     &field, &k, &m, &lb, kern, &us) == 6) {
       const int kk = kernel_from_name(kern);
@@ -258,12 +319,14 @@ fgfc_status fgfc_tune_load(const char* path) {
   std::fclose(f);
   std::lock_guard<std::mutex> lk(g_mu);
   for (const auto& kv : got) g_table[kv.first] = kv.second;
+  for (const auto& kv : tiles) g_tiles[kv.first] = kv.second;
   return clear_error();
 }
 
 void fgfc_tune_clear(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_table.clear();
+  g_tiles.clear();
 }
 
 }  // extern "C"

@@ -38,24 +38,46 @@ impl Batch {
     /// Enqueue every job on `stream`; jobs must not write memory another job reads or writes.
     #[track_caller]
     pub fn run<F: CudaField>(&mut self, jobs: &mut [Job<'_, F>], stream: Stream) {
-        let srcs: Vec<Vec<sys::fgfc_slice>> = jobs.iter().map(|j| j.srcs.iter().map(|s| s.raw()).collect()).collect();
-        let raws: Vec<sys::fgfc_matrix_job> = jobs
-            .iter_mut()
-            .zip(&srcs)
-            .map(|(j, s)| sys::fgfc_matrix_job {
-                plan: j.plan.as_raw(),
-                srcs: s.as_ptr(),
-                nsrcs: s.len(),
-                dst: j.dst.as_mut_ptr(),
-                dst_len: j.dst.len(),
-                row_starts: j.row_starts.as_ref().map_or(ptr::null(), |r| r.as_ptr()),
-                nrows: j.nrows,
-                row_len: j.row_len,
-                overwrite: j.overwrite as i32,
-            })
-            .collect();
+        let srcs = job_slices(jobs);
+        let raws = raw_jobs(jobs, &srcs);
         check(unsafe { sys::fgfc_batch_run(self.raw, raws.as_ptr(), raws.len(), stream.0) });
     }
+
+    /// `fgfc_tune_batch_tiles`: measure the work-list tile shapes on this
+    /// submission (run repeatedly, so its jobs must be safe to rerun) and keep
+    /// the fastest per class; returns the device time in microseconds with the
+    /// starting and with the chosen tiles.
+    #[track_caller]
+    pub fn tune_tiles<F: CudaField>(&mut self, jobs: &mut [Job<'_, F>], stream: Stream) -> (f64, f64) {
+        let srcs = job_slices(jobs);
+        let raws = raw_jobs(jobs, &srcs);
+        let (mut before, mut after) = (0.0, 0.0);
+        check(unsafe {
+            sys::fgfc_tune_batch_tiles(self.raw, raws.as_ptr(), raws.len(), stream.0, &mut before, &mut after)
+        });
+        (before, after)
+    }
+}
+
+fn job_slices<F: CudaField>(jobs: &[Job<'_, F>]) -> Vec<Vec<sys::fgfc_slice>> {
+    jobs.iter().map(|j| j.srcs.iter().map(|s| s.raw()).collect()).collect()
+}
+
+fn raw_jobs<F: CudaField>(jobs: &mut [Job<'_, F>], srcs: &[Vec<sys::fgfc_slice>]) -> Vec<sys::fgfc_matrix_job> {
+    jobs.iter_mut()
+        .zip(srcs)
+        .map(|(j, s)| sys::fgfc_matrix_job {
+            plan: j.plan.as_raw(),
+            srcs: s.as_ptr(),
+            nsrcs: s.len(),
+            dst: j.dst.as_mut_ptr(),
+            dst_len: j.dst.len(),
+            row_starts: j.row_starts.as_ref().map_or(ptr::null(), |r| r.as_ptr()),
+            nrows: j.nrows,
+            row_len: j.row_len,
+            overwrite: j.overwrite as i32,
+        })
+        .collect()
 }
 
 impl Default for Batch {

@@ -265,6 +265,10 @@ extern "C" {
     pub fn fgfc_tune_usable(kernel: fgfc_kernel, field: fgfc_field, nsrcs: usize, nrows: usize) -> c_int;
     pub fn fgfc_tune_shape(field: fgfc_field, nsrcs: usize, nrows: usize, row_len: usize,
                            out: *mut fgfc_kernel) -> fgfc_status;
+    pub fn fgfc_tune_set_tile(elem_bytes: usize, groups: usize, cols: u32) -> fgfc_status;
+    pub fn fgfc_tune_tile(elem_bytes: usize, groups: usize) -> u32;
+    pub fn fgfc_tune_batch_tiles(batch: *mut fgfc_batch, jobs: *const fgfc_matrix_job, njobs: usize,
+                                 stream: fgfc_stream, us_before: *mut f64, us_after: *mut f64) -> fgfc_status;
     pub fn fgfc_tune_save(path: *const c_char) -> fgfc_status;
     pub fn fgfc_tune_load(path: *const c_char) -> fgfc_status;
     pub fn fgfc_tune_clear();

@@ -48,6 +48,16 @@ pub fn tune_shape<F: CudaField>(nsrcs: usize, nrows: usize, row_len: usize) -> K
     Kernel::from_raw(k)
 }
 
+/// Element-vector columns per thread per work item of a batched
+/// split-nibble class (`fgfc_tune_set_tile`: 1, 2, 4, 8 or 16; 0 = built-in).
+pub fn set_tile(elem_bytes: usize, groups: usize, cols: u32) {
+    check(unsafe { sys::fgfc_tune_set_tile(elem_bytes, groups, cols) });
+}
+
+pub fn tile(elem_bytes: usize, groups: usize) -> u32 {
+    unsafe { sys::fgfc_tune_tile(elem_bytes, groups) }
+}
+
 pub fn save(path: &str) {
     let p = CString::new(path).expect("tune::save: path contains NUL");
     check(unsafe { sys::fgfc_tune_save(p.as_ptr()) });

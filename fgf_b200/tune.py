@@ -59,6 +59,30 @@ def tune_shape(field, nsrcs: int, nrows: int, row_len: int) -> str:
     return NAMES[out.value]
 
 
+def set_tile(elem_bytes: int, groups: int, cols: int) -> None:
+    """Element-vector columns per thread per work item of a batched
+    split-nibble class (1, 2, 4, 8 or 16; 0 = built-in)."""
+    check(lib().fgfc_tune_set_tile(elem_bytes, groups, cols))
+
+
+def tile(elem_bytes: int, groups: int) -> int:
+    return int(lib().fgfc_tune_tile(elem_bytes, groups))
+
+
+def tune_batch_tiles(batch, prepared, stream=None) -> tuple[float, float]:
+    """Measure tile shapes on one prepared submission (`batch.Batch`,
+    `batch.Prepared`); returns its device time in microseconds with the
+    starting and with the chosen tiles."""
+    import ctypes as C
+
+    from .ops import _stream
+
+    before, after = C.c_double(), C.c_double()
+    check(lib().fgfc_tune_batch_tiles(batch._h, prepared.array, prepared.n, _stream(stream), C.byref(before),
+                                      C.byref(after)))
+    return before.value, after.value
+
+
 def save(path: str) -> None:
     check(lib().fgfc_tune_save(str(path).encode()))
 

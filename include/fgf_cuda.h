@@ -385,8 +385,27 @@ fgfc_status fgfc_tune_shape(fgfc_field field, size_t nsrcs, size_t nrows, size_t
  * bounded: FGFC_ERR_CUDA if one gave up (its call's results are then not
  * valid), else FGFC_OK. Synchronises with the device; `clear` resets it. */
 fgfc_status fgfc_device_check(int clear);
+/* Tile shape of the batched work lists (fgfc_batch_run and the serving
+ * loop): the 16-byte element vectors each thread takes per work item, for a
+ * split-nibble work-list class (element bytes 1, 2 or 4; table groups 1..4 =
+ * rows per 4-byte group times groups). cols is 1, 2, 4, 8 or 16; 0 restores
+ * the built-in 8. The environment variable FGFC_TILE_COLS (read once)
+ * overrides every class for A/B runs. Tiles change only how work is split,
+ * never the bytes produced. */
+fgfc_status fgfc_tune_set_tile(size_t elem_bytes, size_t groups, unsigned cols);
+unsigned fgfc_tune_tile(size_t elem_bytes, size_t groups);
+/* Measures tile shapes on one submission (run on `stream`, repeatedly: its
+ * jobs must be safe to run again, e.g. overwrite forms): for each
+ * split-nibble class it uses, every tile shape with the other classes fixed,
+ * keeping a shape that is at least 2 % faster; *us_before and *us_after
+ * receive the submission's device time with the starting and the chosen
+ * tiles (either may be NULL). fgfc_tune_save / fgfc_tune_load persist the
+ * tiles with the family table. */
+fgfc_status fgfc_tune_batch_tiles(fgfc_batch *batch, const fgfc_matrix_job *jobs, size_t njobs, fgfc_stream stream,
+                                  double *us_before, double *us_after);
 fgfc_status fgfc_tune_save(const char *path);
 fgfc_status fgfc_tune_load(const char *path);
+/* Forgets measured families and tiles. */
 void fgfc_tune_clear(void);
 
 /* ---------------------------------------------------------------- serving loop */

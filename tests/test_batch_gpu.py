@@ -262,3 +262,47 @@ def _lib_device_ok():
     from fgf_b200 import _lib
 
     return _lib.lib().fgfc_device_check(1) == 0
+
+
+@pytest.mark.parametrize("cols", [1, 2, 4, 16])
+def test_every_tile_shape_gives_the_same_bytes(cuda, cols):
+    """Work-list tile shapes (columns per thread per item) only change how the
+    work is split: the mixed submission matches the oracle under each."""
+    from fgf_b200 import tune
+    try:
+        for E in (1, 2, 4):
+            for G in (1, 2, 3, 4):
+                tune.set_tile(E, G, cols)
+        pool = d(noise(24 << 20, 0xBA7D))
+        jobs, expect = _mixed_jobs(0x200 + cols, pool)
+        fb.Batch().run(jobs)
+        for i, (dst, want) in enumerate(expect):
+            assert np.array_equal(h(dst), want), f"job {i}, {cols} columns per thread"
+    finally:
+        tune.clear()
+
+
+def test_tile_tuner_keeps_results_exact(cuda):
+    """fgfc_tune_batch_tiles reruns an overwrite-only submission under each
+    tile shape and keeps the fastest; the results stay bit-exact."""
+    from fgf_b200 import tune
+    rng = np.random.default_rng(0x711E)
+    jobs, checks = [], []
+    try:
+        for i, (field, k, m, rl) in enumerate([(Gf16, 12, 8, 2 * 40000), (Gf16, 9, 3, 2 * 70001), (Gf8D, 20, 6, 90000),
+                                               (Gf32, 7, 4, 4 * 30000), (Gf8D, 30, 2, 123457)]):
+            vals = [int(x) for x in rng.integers(1, 1 << (8 * field.BYTES), size=k * m, dtype=np.uint64)]
+            srcs_h = [noise(rl, 700 + 10 * i + t) for t in range(k)]
+            want = np.zeros(m * rl, np.uint8)
+            orc.dot_product_matrix(field.ID, want, rl, m, vals, srcs_h)
+            dst = d(noise(m * rl, 799 + i))
+            jobs.append(fb.Job(ops.Plan.matrix(field, k, m, vals), [d(x) for x in srcs_h], dst, rl, m, True))
+            checks.append((dst, want))
+        b = fb.Batch()
+        before, after = tune.tune_batch_tiles(b, b.prepare(jobs))
+        assert before > 0 and after > 0
+        b.run(jobs)
+        for i, (dst, want) in enumerate(checks):
+            assert np.array_equal(h(dst), want), i
+    finally:
+        tune.clear()

@@ -5,6 +5,7 @@ import json
 import pytest
 
 from fgf_b200 import tune
+from fgf_b200._lib import FgfError
 from fgf_b200.fields import Gf8B, Gf8D, Gf16, Gf32
 
 
@@ -54,3 +55,28 @@ def test_table_round_trip(tmp_path):
     tune.save(str(out))
     data = json.loads(out.read_text())
     assert data["entries"] == [{"field": 1, "k": 10, "m": 4, "len_log2": 16, "kernel": "byte", "us": 3.25}]
+
+
+def test_tiles_set_get_and_round_trip(tmp_path):
+    """Work-list tile shapes: built-in 8 columns per thread, settable per
+    (element width, groups) class, persisted beside the family table."""
+    assert tune.tile(2, 4) == 8
+    tune.set_tile(2, 4, 2)
+    tune.set_tile(1, 1, 16)
+    assert (tune.tile(2, 4), tune.tile(1, 1), tune.tile(4, 1)) == (2, 16, 8)
+    p = tmp_path / "tune.json"
+    tune.save(str(p))
+    doc = json.loads(p.read_text())
+    assert sorted((t["elem_bytes"], t["groups"], t["cols"]) for t in doc["tiles"]) == [(1, 1, 16), (2, 4, 2)]
+    tune.clear()
+    assert tune.tile(2, 4) == 8
+    tune.load(str(p))
+    assert (tune.tile(2, 4), tune.tile(1, 1)) == (2, 16)
+    tune.set_tile(2, 4, 0)
+    assert tune.tile(2, 4) == 8
+
+
+@pytest.mark.parametrize("args", [(3, 1, 8), (2, 5, 8), (2, 0, 8), (2, 2, 3), (1, 1, 32)])
+def test_tiles_refuse_unknown_classes_and_shapes(args):
+    with pytest.raises(FgfError):
+        tune.set_tile(*args)
