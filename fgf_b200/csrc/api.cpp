@@ -90,6 +90,7 @@ struct fgfc_plan {
   size_t mat_groups;    // groups per source in the matrix orientation
   size_t off_mat, off_scat, off_gath;  // word offsets into `dev`
   size_t scat_groups, gath_groups;
+  size_t off_k16 = 0, k16_groups = 0;  // Gf16: byte half-product tables of the matrix orientation (batches)
 };
 
 namespace {
@@ -270,10 +271,15 @@ fgfc_status upload_plan_tables(fgfc_plan* p) {
   const size_t n_scat = slots_per_src * p->scat_groups * kCompactWords;
   p->gath_groups = groups(1);
   const size_t n_gath = len * slots_per_src * p->gath_groups * kCompactWords;
-  std::vector<uint32_t> host(n_mat + n_scat + n_gath + 1, 0);
+  // Gf16 batches also run the matrix orientation by byte half-products
+  p->k16_groups = E == 2 ? (p->cols + 3) / 4 : 0;
+  const size_t n_k16 = p->rows * 3 * p->k16_groups * kCompactWords;
+  std::vector<uint32_t> host(n_mat + n_scat + n_gath + n_k16 + 1, 0);
   p->off_mat = 0;
   p->off_scat = n_mat;
   p->off_gath = n_mat + n_scat;
+  p->off_k16 = n_mat + n_scat + n_gath;
+  if (n_k16) build_kara16_tables(p->values.data(), p->cols, p->rows, p->k16_groups, host.data() + p->off_k16);
   if (n_mat) build(p->values.data(), p->cols, p->rows, p->mat_groups, host.data() + p->off_mat);
   if (n_scat) build(p->values.data(), len, 1, p->scat_groups, host.data() + p->off_scat);
   // gather orientation: source i has the single coefficient values[i]
@@ -973,6 +979,31 @@ void lower_tables(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, cons
   }
   const size_t gtot = (nrows + R - 1) / R;
   for (size_t g0 = 0; g0 < gtot; g0 += 4) {
+    const size_t nr = std::min<size_t>(nrows - g0 * R, 4 * R);
+    if (E == 2 && plan->k16_groups && (nr % 4 == 0 || nr % 4 == 3)) {
+      // 3, 4, 7 or 8 rows: byte half-products take 6 lookups per element and
+      // 4 rows where the Gf16 tables take 8 (1 or 2 rows: more; 5 or 6: the same)
+      LoweredJob L;
+      L.field = field;
+      L.kara = true;
+      L.tables = plan->dev + plan->off_k16;
+      L.gstride = plan->k16_groups;
+      L.g0 = g0 * R / 4;
+      L.G = (nr + 3) / 4;
+      L.len = row_len;
+      L.head = head;
+      L.nvec = nvec;
+      L.k = srcs.size();
+      L.nrows = nr;
+      L.ovr = overwrite;
+      L.srcs = srcs;
+      L.dsts.assign(dsts.begin() + g0 * R, dsts.begin() + g0 * R + nr);
+      L.shift = false;
+      if (same && nvec)
+        for (uint64_t d : L.dsts) L.shift = L.shift || (d & 15) != al;
+      out.push_back(std::move(L));
+      continue;
+    }
     LoweredJob L;
     L.field = field;
     L.tables = plan->dev + plan->off_mat;

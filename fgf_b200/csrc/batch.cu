@@ -273,6 +273,183 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------- Gf16 by byte half-products
+
+// Gf16 = Gf8B[u]/(u^2 + u + 0x20) (src/field/gf16.rs:143-153): with
+// c = c0 + c1 u and x = a + b u, A = c0 a, B = c1 b, C = (c0 + c1)(a + b)
+// give c x = (A + 0x20 B) + (A + C) u. Each byte half-product is a Gf8
+// nibble fold whose table word holds 4 rows, so an element costs 3 x 2
+// lookups per 4 rows instead of 2 x 2 per 2 rows. The tables are those of
+// 3 "virtual sources" per source (3t + P, tables.cpp: build_kara16_tables).
+
+// v * 0x20 in every byte of v over Gf8B (x^8 + x^4 + x^3 + x + 1).
+__device__ __forceinline__ uint32_t mul20_4(uint32_t v) {
+#pragma unroll
+  for (int i = 0; i < 5; ++i) v = ((v & 0x7F7F7F7Fu) << 1) ^ (((v >> 7) & 0x01010101u) * 0x1Bu);
+  return v;
+}
+
+// Row word of elements e, e + 1 (lo and hi words: byte r = row 4q + r).
+__device__ __forceinline__ uint32_t k16_word(uint32_t lo0, uint32_t hi0, uint32_t lo1, uint32_t hi1, int r) {
+  const uint32_t sel = static_cast<uint32_t>(r) | ((4u + static_cast<uint32_t>(r)) << 4);
+  return prmt(prmt(lo0, hi0, sel), prmt(lo1, hi1, sel), 0x5410u);
+}
+
+template <int GK, int NE>
+__device__ __forceinline__ void k16_finish(uint32_t (&A)[GK][NE], uint32_t (&B)[GK][NE], uint32_t (&C)[GK][NE]) {
+#pragma unroll
+  for (int q = 0; q < GK; ++q)
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+      B[q][e] = A[q][e] ^ mul20_4(B[q][e]);  // lo
+      C[q][e] ^= A[q][e];                    // hi
+    }
+}
+
+template <int GK, bool SHIFT>
+__device__ void vector_item_k16(const BatchJob& J, const uint64_t* ptrs, uint32_t part, uint32_t t0, uint32_t kk,
+                                bool ovr) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lane4 = lane * 4u;
+  const uint64_t step = static_cast<uint64_t>(J.nv_items) * blockDim.x;
+  for (uint64_t vb = static_cast<uint64_t>(part) * blockDim.x + threadIdx.x - (SHIFT ? lane : 0u); vb < J.nvec;
+       vb += step) {
+    const uint64_t v = SHIFT ? vb + lane : vb;
+    const bool valid = !SHIFT || v < J.nvec;
+    const uint64_t off = J.head + (valid ? v : J.nvec - 1) * 16u;
+    uint32_t A[GK][8], B[GK][8], C[GK][8];
+#pragma unroll
+    for (int q = 0; q < GK; ++q)
+#pragma unroll
+      for (int e = 0; e < 8; ++e) A[q][e] = B[q][e] = C[q][e] = 0;
+    const uint8_t* const* srcs = reinterpret_cast<const uint8_t* const*>(ptrs + J.src_idx + t0);
+    uint4 cur = ldg16(srcs[0] + off);
+    for (uint32_t t = 0; t < kk; ++t) {
+      uint4 nxt = cur;
+      if (t + 1 < kk) nxt = ldg16(srcs[t + 1] + off);
+      // low and high bytes of the 8 elements
+      const uint32_t a0 = prmt(cur.x, cur.y, 0x6420u), a1 = prmt(cur.z, cur.w, 0x6420u);
+      const uint32_t b0 = prmt(cur.x, cur.y, 0x7531u), b1 = prmt(cur.z, cur.w, 0x7531u);
+      const Ctx<1, GK> ca(3u * t, lane4), cb(3u * t + 1u, lane4), cc(3u * t + 2u, lane4);
+      fold<1, GK, 8>(a0, ca, A, 0);
+      fold<1, GK, 8>(a1, ca, A, 4);
+      fold<1, GK, 8>(b0, cb, B, 0);
+      fold<1, GK, 8>(b1, cb, B, 4);
+      fold<1, GK, 8>(a0 ^ b0, cc, C, 0);
+      fold<1, GK, 8>(a1 ^ b1, cc, C, 4);
+      cur = nxt;
+    }
+    k16_finish<GK, 8>(A, B, C);
+#pragma unroll
+    for (int q = 0; q < GK; ++q)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t row = 4 * q + r;
+        uint4 o;
+        o.x = k16_word(B[q][0], C[q][0], B[q][1], C[q][1], r);
+        o.y = k16_word(B[q][2], C[q][2], B[q][3], C[q][3], r);
+        o.z = k16_word(B[q][4], C[q][4], B[q][5], C[q][5], r);
+        o.w = k16_word(B[q][6], C[q][6], B[q][7], C[q][7], r);
+        if constexpr (SHIFT) {
+          const bool rv = valid && row < J.nrows;
+          store_vec16(rv ? reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off : nullptr, o, rv, ovr);
+        } else {
+          if (row < J.nrows) put16(reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off, o, ovr);
+        }
+      }
+  }
+}
+
+// Heads and tails: 4-byte groups (two elements) with byte loads and stores.
+template <int GK>
+__device__ void scalar_item_k16(const BatchJob& J, const uint64_t* ptrs, uint32_t part, uint32_t t0, uint32_t kk,
+                                bool ovr) {
+  const uint32_t lane4 = (threadIdx.x & 31u) * 4u;
+  const uint64_t tail0 = J.head + J.nvec * 16u;
+  const uint64_t n0 = (J.head + 3) / 4, n1 = (J.len - tail0 + 3) / 4;
+  const uint64_t gi = static_cast<uint64_t>(part) * kGroupsPerItem + threadIdx.x;
+  const bool live = gi < n0 + n1;
+  const uint64_t off = !live ? 0 : (gi < n0 ? 4 * gi : tail0 + 4 * (gi - n0));
+  const uint64_t end = !live ? 0 : (gi < n0 ? J.head : J.len);
+  const int nb = !live ? 0 : static_cast<int>(end - off < 4 ? end - off : 4);
+  uint32_t A[GK][4], B[GK][4], C[GK][4];
+#pragma unroll
+  for (int q = 0; q < GK; ++q)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) A[q][e] = B[q][e] = C[q][e] = 0;
+  for (uint32_t t = 0; t < kk; ++t) {
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(ptrs[J.src_idx + t0 + t]) + off;
+    uint32_t w = 0;
+    for (int b = 0; b < nb; ++b) w |= static_cast<uint32_t>(s[b]) << (8 * b);
+    const uint32_t a = prmt(w, 0u, 0x4420u), bb = prmt(w, 0u, 0x4431u);  // [a0 a1 0 0], [b0 b1 0 0]
+    const Ctx<1, GK> ca(3u * t, lane4), cb(3u * t + 1u, lane4), cc(3u * t + 2u, lane4);
+    fold<1, GK, 4>(a, ca, A, 0);
+    fold<1, GK, 4>(bb, cb, B, 0);
+    fold<1, GK, 4>(a ^ bb, cc, C, 0);
+  }
+  if (!live) return;
+  k16_finish<GK, 4>(A, B, C);
+#pragma unroll
+  for (int q = 0; q < GK; ++q)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint32_t row = 4 * q + r;
+      if (row >= J.nrows) continue;
+      const uint32_t o = k16_word(B[q][0], C[q][0], B[q][1], C[q][1], r);
+      uint8_t* d = reinterpret_cast<uint8_t*>(ptrs[J.dst_idx + row]) + off;
+      for (int b = 0; b < nb; ++b) {
+        const uint8_t v = static_cast<uint8_t>(o >> (8 * b));
+        d[b] = ovr ? v : static_cast<uint8_t>(d[b] ^ v);
+      }
+    }
+}
+
+// Persistent work-list kernel of a Gf16 half-product class: GK row quads.
+template <int GK, bool SHIFT>
+__global__ void __launch_bounds__(kThreads, 1)
+    batch_kernel_k16(const BatchJob* __restrict__ jobs, const uint64_t* __restrict__ ptrs,
+                     const uint2* __restrict__ items, uint32_t nitems, uint32_t* counter) {
+  __shared__ uint32_t s_item;
+  __shared__ const uint32_t* s_tab;
+  __shared__ uint32_t s_g0, s_t0;
+  const uint32_t kc = kMaxSlots / (3 * GK);  // sources whose tables fit at once
+  if (threadIdx.x == 0) {
+    s_tab = nullptr;
+    s_g0 = s_t0 = 0xFFFFFFFFu;
+  }
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, kClaim);
+    __syncthreads();
+    const uint32_t first = s_item;
+    if (first >= nitems) break;
+    for (uint32_t it = first; it < first + kClaim && it < nitems; ++it) {
+      const uint2 wi = items[it];
+      const BatchJob J = jobs[wi.x];
+      const uint32_t nchunks = (J.k + kc - 1) / kc;
+      for (uint32_t c = 0; c < nchunks; ++c) {
+        const uint32_t t0 = c * kc, kk = min(kc, J.k - t0);
+        __syncthreads();
+        const bool resident = s_tab == J.tables && s_g0 == J.g0 && s_t0 == t0;
+        if (!resident) {
+          fill_chunk<1, GK>(J, 3 * t0, 3 * kk);
+          if (threadIdx.x == 0) {
+            s_tab = J.tables;
+            s_g0 = J.g0;
+            s_t0 = t0;
+          }
+        }
+        const bool ovr = J.ovr && c == 0;
+        if (wi.y < J.nv_items)
+          vector_item_k16<GK, SHIFT>(J, ptrs, wi.y, t0, kk, ovr);
+        else
+          scalar_item_k16<GK>(J, ptrs, wi.y - J.nv_items, t0, kk, ovr);
+        __syncthreads();  // chunk c's writes precede chunk c + 1's reads of the same rows
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- byte-table classes
 
 // Work-list kernel for Gf8 sub-jobs of at most 4 rows and exactly K sources.
@@ -593,6 +770,12 @@ KernelFn kernel_for_s(int E, int G) {
 
 KernelFn kernel_for(int E, int G, bool shift) { return shift ? kernel_for_s<true>(E, G) : kernel_for_s<false>(E, G); }
 
+KernelFn kernel_for_k16(int GK, bool shift) {
+  if (GK == 1) return shift ? batch_kernel_k16<1, true> : batch_kernel_k16<1, false>;
+  if (GK == 2) return shift ? batch_kernel_k16<2, true> : batch_kernel_k16<2, false>;
+  return nullptr;
+}
+
 #define FGFC_K_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
 
 KernelFn fast_kernel_for(int K, bool shift) {
@@ -650,6 +833,7 @@ struct BatchClass {
   std::vector<uint64_t> seg_prefix; // and the prefix of their vector counts (the segmented launch)
   bool uniform = false;        // byte-table class whose sub-jobs share one plan
   bool shift = false;          // its rows are not all at the sources' offset within 16 bytes
+  bool kara = false;           // Gf16 by byte half-products, G = row quads
 };
 
 // Descriptor slots used round robin: a submission waits (on the host) only
@@ -791,9 +975,12 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
     const LoweredJob& L = jobs[i];
     const int E = field_bytes(L.field);
     const bool fast = E == 1 && L.G == 1 && L.k >= 1 && L.k <= static_cast<size_t>(kFastMaxK);
-    const int key = (fast ? 100 + static_cast<int>(L.k) : E * 8 + static_cast<int>(L.G)) + (L.shift ? 300 : 0);
+    const int key = (fast ? 100 + static_cast<int>(L.k) : L.kara ? 200 + static_cast<int>(L.G)
+                                                                  : E * 8 + static_cast<int>(L.G)) +
+                    (L.shift ? 300 : 0);
     BatchClass& c = classes[key];
     c.shift = L.shift;
+    c.kara = L.kara;
     c.E = E;
     c.G = static_cast<int>(L.G);
     c.K = fast ? static_cast<int>(L.k) : 0;
@@ -969,7 +1156,7 @@ cudaError_t batch_run(void* state, const std::vector<LoweredJob>& jobs, const st
     if (c.uniform) {
       L.ufn = uniform_kernel_for(c.K, c.shift);
     } else {
-      L.fn = fast ? fast_kernel_for(c.K, c.shift) : kernel_for(c.E, c.G, c.shift);
+      L.fn = fast ? fast_kernel_for(c.K, c.shift) : c.kara ? kernel_for_k16(c.G, c.shift) : kernel_for(c.E, c.G, c.shift);
     }
     if (!L.fn && !L.ufn) return cudaErrorInvalidValue;
     L.smem = fast ? fast_smem(c.K) : static_cast<uint32_t>(kBatchSmem);

@@ -60,6 +60,11 @@ void build_compact_tables(int field, const uint64_t* coeffs, size_t m, size_t t0
 // [((t * 3 + P) * 4 + p) * M + j][32]: product P (A, B, C), input byte p of
 // the 4-byte half, 16 words for its low nibble and 16 for its high nibble.
 constexpr size_t kWideSlotsPerSrcRow = 12;
+// The same split for Gf16 = Gf8B[u]/(u^2 + u + 0x20): lo = A + 0x20 B,
+// hi = A + C over byte half-products. Tables for the batched work lists:
+// [(t * 3 + P) * Gq + q][32], nibble tables whose word holds the byte
+// half-product P of rows 4q .. 4q + 3 (zero past m); Gq = ceil(m / 4).
+void build_kara16_tables(const uint64_t* coeffs, size_t m, size_t k, size_t Gq, uint32_t* out);
 void build_wide_tables(int field, const uint64_t* coeffs, size_t m, size_t t0, size_t k, size_t j0, size_t M,
                        uint32_t* out);
 // The fix-up map of an 8-byte field as [4 input bytes][32] nibble tables:
@@ -129,6 +134,7 @@ struct LoweredJob {
   size_t k, nrows;
   bool ovr;
   bool shift;              // some row is not at the sources' offset within 16 bytes
+  bool kara = false;       // Gf16 by byte half-products (tables: build_kara16_tables; G = row quads)
   std::vector<uint64_t> srcs, dsts;
 };
 

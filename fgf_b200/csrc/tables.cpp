@@ -105,4 +105,26 @@ void build_wide_fixup(int field, uint32_t* out) {
   linear_tables(img, out, 1);
 }
 
+void build_kara16_tables(const uint64_t* coeffs, size_t m, size_t k, size_t Gq, uint32_t* out) {
+  for (size_t t = 0; t < k; ++t)
+    for (int P = 0; P < 3; ++P)
+      for (size_t q = 0; q < Gq; ++q) {
+        uint8_t cp[4];
+        for (int r = 0; r < 4; ++r) {
+          const size_t j = 4 * q + r;
+          const uint64_t c = j < m ? coeffs[t * m + j] : 0;
+          const uint8_t c0 = static_cast<uint8_t>(c), c1 = static_cast<uint8_t>(c >> 8);
+          cp[r] = P == 0 ? c0 : P == 1 ? c1 : static_cast<uint8_t>(c0 ^ c1);
+        }
+        uint32_t* slot = out + ((t * 3 + P) * Gq + q) * kCompactWords;
+        for (int half = 0; half < 2; ++half)
+          for (int n = 0; n < 16; ++n) {
+            const uint8_t x = static_cast<uint8_t>(half ? (n << 4) : n);
+            uint32_t w = 0;
+            for (int r = 0; r < 4; ++r) w |= static_cast<uint32_t>(gf8b_mul(cp[r], x)) << (8 * r);
+            slot[half * 16 + n] = w;
+          }
+      }
+}
+
 }  // namespace fgfc

@@ -306,3 +306,50 @@ def test_tile_tuner_keeps_results_exact(cuda):
             assert np.array_equal(h(dst), want), i
     finally:
         tune.clear()
+
+
+@pytest.mark.parametrize("m", [3, 4, 7, 8, 11, 16])
+def test_gf16_half_product_classes(cuda, m):
+    """Gf16 stripes with 3, 4, 7 or 8 rows per 8-row sub-job run on byte
+    half-products (lo = A + 0x20 B, hi = A + C): unaligned heads and ragged
+    tails (scalar items), rows off the sources' 16-byte offset (shifted
+    stores), accumulate and overwrite, more sources than one table pass."""
+    rng = np.random.default_rng(0x16A + m)
+    pool = d(noise(16 << 20, 0x16B + m))
+    host = h(pool)
+    jobs, checks = [], []
+    cur = 256
+    for i, (k, rl, src_skew, dst_skew, ovr, scattered) in enumerate([
+            (5, 2 * 20011, 0, 0, True, False), (23, 2 * 9000 + 6, 4, 4, True, False),
+            (12, 2 * 7777, 2, 10, False, False), (30, 2 * 4099, 0, 6, True, True), (3, 2 * 33, 6, 0, False, False)]):
+        vals = [int(x) for x in rng.integers(0, 1 << 16, size=k * m, dtype=np.uint64)]
+        s_off = []
+        for t in range(k):
+            s_off.append(cur + src_skew)
+            cur += (rl + 64 + 255) // 256 * 256
+        srcs_h = [host[o:o + rl].copy() for o in s_off]
+        plan = ops.Plan.matrix(Gf16, k, m, vals)
+        if scattered:
+            stride = rl + 2 * 7
+            base = cur + dst_skew
+            cur += (stride * m + 511) // 256 * 256
+            starts = [j * stride for j in range(m)][::-1]
+            dst = pool[base:base + stride * m]
+            want = host[base:base + stride * m].copy()
+            if ovr:
+                for j, st in enumerate(starts):
+                    want[st:st + rl] = 0
+            orc.mul_add_matrix_scattered(Gf16.ID, want, rl, starts, vals, srcs_h)
+            jobs.append(fb.Job(plan, [pool[o:o + rl] for o in s_off], dst, rl, m, ovr, starts))
+        else:
+            base = cur + dst_skew
+            cur += (rl * m + 511) // 256 * 256
+            dst = pool[base:base + rl * m]
+            want = host[base:base + rl * m].copy()
+            (orc.dot_product_matrix if ovr else orc.mul_add_matrix)(Gf16.ID, want, rl, m, vals, srcs_h)
+            jobs.append(fb.Job(plan, [pool[o:o + rl] for o in s_off], dst, rl, m, ovr))
+        checks.append((dst, want))
+        assert cur < pool.numel()
+    fb.Batch().run(jobs)
+    for i, (dst, want) in enumerate(checks):
+        assert np.array_equal(h(dst), want), f"job {i}, m = {m}"
