@@ -1212,7 +1212,7 @@ CASES = {
     "rs104_encode": ("Gf8D", 10, 4), "gf16_rs8_2": ("Gf16", 8, 2),
     "gf64_rs104": ("Gf64", 10, 4), "fp64_rs104": ("FanPaar64", 10, 4),
     "axpy": "mul_add", "scatter": "mul_add_scatter", "gather": "mul_add_gather",
-    "xor": "add_assign", "elementwise": "mul_elementwise", "uneven": "uneven",
+    "xor": "add_assign", "elementwise": "mul_elementwise", "uneven": "uneven", "batch_gf16_12_8": "batch16",
 }
 
 
@@ -1249,6 +1249,30 @@ def run_case(args):
         ok = oracle_matrix_windows(field.ID, srcs, None, [rows[j * n:(j + 1) * n] for j in range(m)], vals, True, rng)
         alg, src_b = (k + m) * n, k * n
         kernel = "wide" if field.BYTES == 8 else tune.chosen(field, k, m, n)
+    elif spec == "batch16":
+        # one batched submission of 64 Gf16 stripes, 12 sources and 8 rows of
+        # case-mib MiB each, every stripe its own plan
+        from fgf_b200 import batch as fb
+        field, k, m, ns = fields.Gf16, 12, 8, 64
+        n -= n % 2
+        buf = torch.randint(0, 256, (ns * (k + m) * n,), dtype=torch.uint8, device=dev, generator=g)
+        jobs, chk = [], []
+        for s_ in range(ns):
+            vals = [int(x) for x in rng.integers(1, 1 << 16, size=k * m, dtype=np.uint64)]
+            base = s_ * (k + m) * n
+            srcs = [buf[base + t * n:base + (t + 1) * n] for t in range(k)]
+            rows = buf[base + k * n:base + (k + m) * n]
+            jobs.append(fb.Job(ops.Plan.matrix(field, k, m, vals), srcs, rows, n, m, True))
+            chk.append((srcs, rows, vals))
+        bt = fb.Batch(graphs=True)
+        prep = bt.prepare(jobs)
+        fn = lambda: bt.run_prepared(prep, stream)
+        fn()
+        torch.cuda.synchronize()
+        ok = all(oracle_matrix_windows(field.ID, chk[i][0], None, [chk[i][1][j * n:(j + 1) * n] for j in range(m)],
+                                       chk[i][2], True, rng) for i in (0, ns // 2, ns - 1))
+        alg, src_b = ns * (k + m) * n, ns * k * n
+        kernel = "batch (Gf16 half-products)" if os.environ.get("FGFC_GF16_HALF", "1") != "0" else "batch (Gf16 tables)"
     elif spec == "uneven":
         res = uneven_batch(dev, max(16, int(args.case_mib)), max(1, args.steps))
         print(json.dumps({"case": args.case, **res}))

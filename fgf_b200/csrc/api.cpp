@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -980,7 +981,13 @@ void lower_tables(const fgfc_plan* plan, const std::vector<uint64_t>& srcs, cons
   const size_t gtot = (nrows + R - 1) / R;
   for (size_t g0 = 0; g0 < gtot; g0 += 4) {
     const size_t nr = std::min<size_t>(nrows - g0 * R, 4 * R);
-    if (E == 2 && plan->k16_groups && (nr % 4 == 0 || nr % 4 == 3)) {
+    // FGFC_GF16_HALF=0 in the environment (read once) keeps every Gf16
+    // sub-job on the Gf16 tables, for A/B runs
+    static const bool half_on = [] {
+      const char* v = std::getenv("FGFC_GF16_HALF");
+      return !(v && v[0] == '0');
+    }();
+    if (half_on && E == 2 && plan->k16_groups && (nr % 4 == 0 || nr % 4 == 3)) {
       // 3, 4, 7 or 8 rows: byte half-products take 6 lookups per element and
       // 4 rows where the Gf16 tables take 8 (1 or 2 rows: more; 5 or 6: the same)
       LoweredJob L;
