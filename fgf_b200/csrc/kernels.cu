@@ -443,24 +443,24 @@ __device__ __forceinline__ void gmul16x2_pair(uint32_t x1, uint32_t y1, uint32_t
   const uint32_t xs = prmt(x1 ^ (x1 >> 8), x2 ^ (x2 >> 8), 0x6420u);      // a + b of the 4 elements
   const uint32_t ys = prmt(y1 ^ (y1 >> 8), y2 ^ (y2 >> 8), 0x6420u);
   const uint32_t q = gmul4<0x1Bu>(xs, ys);                                 // (a+b)(c+d) of the 4 elements
-  uint32_t c1 = p1, c2 = p2;                                               // 0x20 * p: five doublings
+  uint32_t c = prmt(p1, p2, 0x7531u);                                      // the 4 bd, then 0x20 bd:
 #pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    c1 = xtime4<0x1Bu>(c1);
-    c2 = xtime4<0x1Bu>(c2);
-  }
-  r1 = prmt(p1, p1, 0x2200u) ^ prmt(c1, q, 0x5341u);
-  r2 = prmt(p2, p2, 0x2200u) ^ prmt(c2, q, 0x7361u);
+  for (int i = 0; i < 5; ++i) c = xtime4<0x1Bu>(c);                        // five doublings
+  r1 = prmt(p1, p1, 0x2200u) ^ prmt(c, q, 0x5140u);
+  r2 = prmt(p2, p2, 0x2200u) ^ prmt(c, q, 0x7362u);
 }
 
 // 0x2000 times each Gf16 lane (a + b u) of a word: 0x20 0x20 b + 0x20 (a + b) u.
+// The hi lanes (a + b) take 5 doublings and the lo lanes (b) 10: the first 5
+// run on both at once.
 __device__ __forceinline__ uint32_t gmul2000x2(uint32_t v) {
-  uint32_t hi = (v ^ (v << 8)) & 0xFF00FF00u, lo = (v >> 8) & 0x00FF00FFu;
+  uint32_t w = ((v ^ (v << 8)) & 0xFF00FF00u) | ((v >> 8) & 0x00FF00FFu);
 #pragma unroll
-  for (int i = 0; i < 5; ++i) hi = xtime4<0x1Bu>(hi);
+  for (int i = 0; i < 5; ++i) w = xtime4<0x1Bu>(w);
+  uint32_t lo = w & 0x00FF00FFu;
 #pragma unroll
-  for (int i = 0; i < 10; ++i) lo = xtime4<0x1Bu>(lo);
-  return hi | lo;
+  for (int i = 0; i < 5; ++i) lo = xtime4<0x1Bu>(lo);
+  return (w & 0xFF00FF00u) | lo;
 }
 
 // One Gf32 product per word: [A, B] as Gf16 halves.
