@@ -73,6 +73,28 @@ def erasure_patterns(nst: int, seed: int = 0x5EED):
     return [tuple(sorted(rng.choice(N_ALL, size=M_PAR, replace=False).tolist())) for _ in range(nst)]
 
 
+def rank_seeds(rank: int) -> tuple[int, int]:
+    """Seeds of a rank's own stripes (data, erasure patterns): under torchrun
+    every rank encodes and rebuilds its own batch (weak scaling)."""
+    return 0x1234 + rank, 0x5EED + rank
+
+
+def max_over_ranks(ms: float, dist=None, device=None) -> float:
+    """The slowest rank's time: the job ends when its last rank does."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_source_gbps(src_bytes_per_rank_step: int, world: int, ms_per_step: float) -> float:
+    """Whole-job source GB/s: every rank's bytes over the slowest rank's time."""
+    return src_bytes_per_rank_step * world / (ms_per_step / 1e3) / 1e9
+
+
 def config(args, L):
     return {
         "workload": f"RS(10,4) Gf8D, {args.stripes} stripes x {L >> 10} KiB shards: batched encode "
@@ -913,11 +935,12 @@ def run_ours(args):
     stripe = N_ALL * L
     code = torch.empty(nst * stripe, dtype=torch.uint8, device=dev)
     g = torch.Generator(device=dev)
-    g.manual_seed(0x1234 + rank)
+    data_seed, pattern_seed = rank_seeds(rank)
+    g.manual_seed(data_seed)
     code.random_(0, 256, generator=g)
     cm = cauchy(Gf8D, M_PAR, K_SRC)
     enc_plan = ops.Plan.matrix(Gf8D, *encode_plan_coeffs(cm))
-    pats = erasure_patterns(nst, seed=0x5EED + rank)
+    pats = erasure_patterns(nst, seed=pattern_seed)
     cache = {}
 
     def dec_plan(er):
@@ -1001,13 +1024,11 @@ def run_ours(args):
     enc_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / args.steps
     rec_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / args.steps
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
         dist.barrier()
     ms_step = ms / args.steps
     src_per_step = nst * 2 * K_SRC * L * world
-    value = src_per_step / (ms_step / 1e3) / 1e9
+    value = job_source_gbps(nst * 2 * K_SRC * L, world, ms_step)
 
     # ---- roofline of the dominant kernels (byte-table batch kernels, K = 10)
     peak, peak_kind = hbm_peak()
@@ -1133,9 +1154,7 @@ def run_ours(args):
         ems = e0.elapsed_time(e1)
         same = bool(torch.equal(host_out, want_out))
         if dist:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+            ems = max_over_ranks(ems, dist, dev)
         h2d, d2h = nst * dsz, nst * osz
         bound_ms = max(h2d / pcie["h2d_GB/s"], d2h / pcie["d2h_GB/s"]) / 1e6
         e2e = {"value": round(src_per_step / (ems / es / 1e3) / 1e9, 2), "unit": "GB/s",
