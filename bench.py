@@ -285,6 +285,62 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every ~2 ms during
+    the timed region (reading only; nothing is set). The nvidia-smi loop
+    above starts too slowly to sample a region of a few tens of ms."""
+
+    def __init__(self, dev):
+        import threading
+
+        import pynvml as nv
+        import torch
+
+        self.nv = nv
+        nv.nvmlInit()
+        pr = torch.cuda.get_device_properties(dev)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        self.rows = []
+        self.stop_ev = threading.Event()
+        self.first = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self.nv
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop_ev.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.rows.append((mhz, sorted(n for n, b in bits.items() if rs & b)))
+            except Exception:
+                pass
+            self.first.set()
+            time.sleep(0.002)
+
+    def start(self):
+        self.thread.start()
+        self.first.wait(timeout=2.0)
+
+    def stop(self):
+        self.stop_ev.set()
+        self.thread.join(timeout=2.0)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.rows:
+            return None
+        reasons = sorted({r for _, rs in self.rows for r in rs})
+        return {"sm_mhz": float(np.median([m for m, _ in self.rows])), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml, every ~2 ms"}
+
+
 def hbm_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -1001,7 +1057,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    sampler = ClockSampler(local)
+    try:
+        sampler = NvmlClockSampler(dev)
+    except Exception:  # no NVML: the nvidia-smi loop
+        sampler = ClockSampler(local)
     sampler.start()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     start = torch.cuda.Event(enable_timing=True)
