@@ -1237,12 +1237,9 @@ def run_ours(args):
     if world == 1 and not args.no_legs:
         legs = {"config0_single_stripe_64KiB": leg_single_stripe(dev)}
         torch.cuda.empty_cache()
-        # the 256 MiB single-row ops run before the 56 GiB leg: measured after
-        # it (fresh allocations once that memory is released) they ran at
-        # 0.6 of HBM instead of 0.85-0.93 standalone
-        legs["config1_single_row_256MiB"] = leg_single_row_ops(dev)
-        torch.cuda.empty_cache()
         legs["config1_64MiB_shards"] = leg_64mib(dev, args.c1_stripes)
+        torch.cuda.empty_cache()
+        legs["config1_single_row_256MiB"] = leg_single_row_ops(dev)
         torch.cuda.empty_cache()
         legs["config2_tower_large_km"] = leg_tower_and_large_km(dev)
         legs["fields_64bit_rs10_4"] = leg_wide_fields(dev)
