@@ -586,26 +586,43 @@ __global__ void elementwise_fp_kernel(uint8_t* __restrict__ dst, const uint8_t* 
   }
 }
 
+// 0x20000000 times a Gf32 element [A, B] (Gf16 halves): v = 0x2000 in the
+// high half, so (A + B v) 0x2000 v = 0x2000 0x2000 B + 0x2000 (A + B) v.
+__device__ __forceinline__ uint32_t gmul20000000(uint32_t w) {
+  const uint32_t u = ((w ^ (w << 16)) & 0xFFFF0000u) | (w >> 16);  // [B, A + B]
+  const uint32_t u1 = gmul2000x2(u);                                 // [0x2000 B, 0x2000 (A + B)]
+  return (u1 & 0xFFFF0000u) | (gmul2000x2(u1) & 0x0000FFFFu);
+}
+
+__device__ __forceinline__ uint64_t ld8(const uint8_t* p) {
+  if ((reinterpret_cast<uintptr_t>(p) & 7u) == 0) return *reinterpret_cast<const uint64_t*>(p);
+  uint64_t v = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v |= static_cast<uint64_t>(p[k]) << (8 * k);
+  return v;
+}
+
 // GF(2^64) = Gf32[w]/(w^2 + w + 0x20000000): three word-parallel Gf32
-// products and one product by the constant (src/field/gf64.rs:120-128).
+// products and one product by the constant (src/field/gf64.rs:120-128),
+// that one by doublings.
 __global__ void elementwise_gf64_kernel(uint8_t* __restrict__ dst, const uint8_t* __restrict__ a,
                                         const uint8_t* __restrict__ b, uint64_t nelem) {
   const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nelem; i += stride) {
-    uint64_t x = 0, y = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      x |= static_cast<uint64_t>(a[8 * i + k]) << (8 * k);
-      y |= static_cast<uint64_t>(b[8 * i + k]) << (8 * k);
-    }
+    const uint64_t x = ld8(a + 8 * i), y = ld8(b + 8 * i);
     const uint32_t p = static_cast<uint32_t>(x), q = static_cast<uint32_t>(x >> 32);
     const uint32_t c = static_cast<uint32_t>(y), d = static_cast<uint32_t>(y >> 32);
     const uint32_t ac = gmul32(p, c), bd = gmul32(q, d);
-    const uint32_t lo = ac ^ gmul32(bd, 0x20000000u);
+    const uint32_t lo = ac ^ gmul20000000(bd);
     const uint32_t hi = gmul32(p ^ q, c ^ d) ^ ac;
     const uint64_t r = static_cast<uint64_t>(lo) | (static_cast<uint64_t>(hi) << 32);
+    uint8_t* o = dst + 8 * i;
+    if ((reinterpret_cast<uintptr_t>(o) & 7u) == 0) {
+      *reinterpret_cast<uint64_t*>(o) = r;
+    } else {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) dst[8 * i + k] = static_cast<uint8_t>(r >> (8 * k));
+      for (int k = 0; k < 8; ++k) o[k] = static_cast<uint8_t>(r >> (8 * k));
+    }
   }
 }
 
