@@ -37,13 +37,15 @@ def _buf(x) -> tuple[int, int]:
     """(device pointer, byte length) of a device buffer."""
     if isinstance(x, tuple):
         return int(x[0]), int(x[1])
-    if hasattr(x, "data_ptr"):
-        if not x.is_cuda:
-            raise TypeError("fgf_b200.ops: buffers must be device (CUDA) memory")
-        if not x.is_contiguous():
-            raise TypeError("fgf_b200.ops: buffers must be contiguous")
-        return int(x.data_ptr()), int(x.numel() * x.element_size())
-    raise TypeError(f"fgf_b200.ops: unsupported buffer type {type(x).__name__}")
+    try:
+        on_device = x.is_cuda
+    except AttributeError:
+        raise TypeError(f"fgf_b200.ops: unsupported buffer type {type(x).__name__}") from None
+    if not on_device:
+        raise TypeError("fgf_b200.ops: buffers must be device (CUDA) memory")
+    if not x.is_contiguous():
+        raise TypeError("fgf_b200.ops: buffers must be contiguous")
+    return x.data_ptr(), x.nbytes
 
 
 def _stream(stream) -> int:
@@ -78,10 +80,21 @@ def _wide(field) -> bool:
     return FIELDS[_fid(field)].BYTES == 8
 
 
-def _slices(srcs: Sequence) -> tuple[C.Array, int]:
-    bufs = [_buf(s) for s in srcs]
-    arr = (Slice * max(1, len(bufs)))(*[Slice(p, n) for p, n in bufs])
-    return arr, len(bufs)
+_SLICE_WORDS: dict = {}
+
+
+def _slices(srcs: Sequence):
+    """fgfc_slice array of the sources: built as one flat array of (pointer,
+    length) words (one ctypes object instead of one per source) and viewed
+    as the struct array, which keeps the words alive."""
+    flat = []
+    for s in srcs:
+        flat.extend(_buf(s))
+    n = len(flat) // 2
+    typ = _SLICE_WORDS.get(n)
+    if typ is None:
+        typ = _SLICE_WORDS[n] = C.c_uint64 * max(2, 2 * n)
+    return C.cast(typ(*flat), C.POINTER(Slice)), n
 
 
 def _terms(terms: Sequence) -> tuple[C.Array, int, list]:
