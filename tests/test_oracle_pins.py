@@ -319,3 +319,15 @@ def test_wide_oracle_ops_agree_with_the_scalar_product(fid):
         for i, v in enumerate(srcs[t].view("<u8")):
             want[i] ^= np.uint64(orc.mul64(fid, c[t], int(v)))
     assert np.array_equal(got.view("<u8"), want)
+
+
+def test_gf16_mul_add_doctest():
+    """src/lib.rs:53-65: mul_add over Gf16's little-endian bytes equals the
+    field product written back as bytes."""
+    v = GOLD["gf16_mul_add_doctest"]
+    src = np.frombuffer(bytes.fromhex(v["src_le"]), np.uint8).copy()
+    dst = np.frombuffer(bytes.fromhex(v["dst0"]), np.uint8).copy()
+    coeff = int(v["coeff"], 16)
+    orc.mul_add(orc.GF16, dst, coeff, src)
+    prod = orc.mul(orc.GF16, int.from_bytes(src.tobytes(), "little"), coeff)
+    assert dst.tobytes() == prod.to_bytes(2, "little") == bytes.fromhex(v["product_le"])
